@@ -1,0 +1,425 @@
+"""Benchmark of the MP-PCA denoiser hot path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--form plain|accurate] [--workload headline|config1]
+
+A step is one denoise of one synthetic volume already resident in HBM: the
+headline workload is 96x96x48x48 (x, y, z, t) with 11^3 patches at stride 3
+(12600 patches of 1331 x 48), rank-4 signal in [0, 1] plus N(0, 0.05^2) noise.
+``value`` is whole-job patches/s from CUDA events around each step (L2 flushed
+by a 256 MiB write between steps, outside the events); ``e2e`` is the same
+metric through the C ABI's host-buffer call (pinned host in/out, both copies
+inside the timed region). Under torchrun every rank denoises its own volume
+(independent objects: weak scaling, no data-path collective); the step time is
+the max over ranks.
+
+``--impl reference`` times the reference algorithm's CPU implementation (the
+step-0 NumPy loop restated in oracle/, all host cores through a spawn pool)
+on a bounded sample of the same workload's patches.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "headline": dict(shape=(96, 96, 48, 48), patch=(11, 11, 11), stride=3,
+                     desc="96x96x48x48 volume, 11^3 patches, stride 3 (12600 patches of 1331x48)"),
+    "config1": dict(shape=(48, 48, 24, 48), patch=(11, 11, 11), stride=3,
+                    desc="48x48x24x48 volume, 11^3 patches, stride 3 (1176 patches of 1331x48)"),
+}
+PUBLISHED_STEP8_MS = 66.5  # reference step 8, host->host best of 5, 12600 patches (README.md:48)
+PHASE_KERNEL = {"center": "center_kernel", "gram": "gram_kernel", "eigh_mp": "eigh_mp_kernel",
+                "recon": "recon_kernel"}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--form", choices=["plain", "accurate"], default="plain")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="headline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="patches in the CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+# ----------------------------------------------------------------------------- CPU side
+def cpu_step0_rate(vol, patch, stride, n_patches_sample, processes):
+    """Patches/s of the step-0 loop (oracle port) over a sample of the corner
+    list, spread over ``processes`` spawn workers with one BLAS thread each.
+
+    Each worker receives the volume once (pool initializer) and runs the
+    step-0 per-patch work - gather, centre, SVD, MP rank, reconstruct, weighted
+    accumulate into its own ``out``/``wsum`` - over its share of the sample;
+    the wall time of that loop across the pool is the measurement.
+    """
+    import multiprocessing as mp
+
+    from oracle import mppca as orc
+
+    corners = orc.patch_corners(vol.shape, patch, stride)
+    sample = corners[np.linspace(0, len(corners) - 1, n_patches_sample).astype(int)]
+    chunks = [c for c in np.array_split(sample, processes) if len(c)]
+    for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
+        os.environ[k] = "1"
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(len(chunks), initializer=_cpu_init, initargs=(vol, patch)) as pool:
+        pool.map(_cpu_worker, [c[:1] for c in chunks])  # warm (imports, first SVD)
+        t0 = time.perf_counter()
+        pool.map(_cpu_worker, chunks)
+        dt = time.perf_counter() - t0
+    return len(sample) / dt, dt, len(chunks)
+
+
+_CPU = {}
+
+
+def _cpu_init(vol, patch):
+    _CPU["vol"] = vol
+    _CPU["patch"] = patch
+    _CPU["out"] = np.zeros_like(vol)
+    _CPU["wsum"] = np.zeros(vol.shape[:3] + (1,), dtype=vol.dtype)
+
+
+def _cpu_worker(corners):
+    from oracle import mppca as orc
+
+    vol, (px, py, pz) = _CPU["vol"], _CPU["patch"]
+    out, wsum = _CPU["out"], _CPU["wsum"]
+    for i, j, k in corners:
+        sl = np.s_[i:i + px, j:j + py, k:k + pz]
+        xd, p = orc.mppca_patch(vol[sl].reshape(-1, vol.shape[-1]))
+        w = 1.0 / (2.0 + p)
+        out[sl] += w * xd.reshape(px, py, pz, -1)
+        wsum[sl] += w
+    return len(corners)
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, wl):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    vol, _ = make_phantom_lowrank(wl["shape"], seed=0)
+    cores = host_cores()
+    per_step = args.cpu_sample or max(64, 48 * cores)
+    for _ in range(args.warmup):
+        cpu_step0_rate(vol, wl["patch"], wl["stride"], min(per_step, cores * 4), cores)
+    rates = []
+    for _ in range(args.steps):
+        r, _, used = cpu_step0_rate(vol, wl["patch"], wl["stride"], per_step, cores)
+        rates.append(r)
+    from lowrank_gpu_fastest_b200.problem import n_patches
+
+    P = n_patches(wl["shape"], wl["patch"], wl["stride"])
+    value = float(statistics.mean(rates))
+    line = dict(
+        impl="reference", metric="patches_per_s", value=value, unit="patches/s", n_gpus=args.gpus,
+        steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * per_step / value,
+        ms_per_volume=1e3 * P / value, higher_is_better=True, scaling="weak", vs_baseline=None,
+        dtype="f32", data="synthetic",
+        config=dict(workload=wl["desc"], shape=list(wl["shape"]), patch=list(wl["patch"]),
+                    stride=wl["stride"], phantom="rank-4 [0,1] + N(0,0.05^2), seed 0"),
+        cpu_baseline=dict(value=value, unit="patches/s", cores=used, kind="port",
+                          sample=f"{per_step} patches per step, evenly spaced over the {P}-patch corner "
+                                 f"list; step-0 NumPy loop (SVD + MP rank + weighted accumulate), one BLAS "
+                                 f"thread per spawn worker"),
+        e2e=dict(value=value, unit="patches/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+    )
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU side
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return dict(sm_mhz=statistics.median(sms) if sms else None, sm_max_mhz=mx,
+                    reasons=sorted(reasons), samples=len(sms),
+                    power_w_max=max(power) if power else None)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return dict(hbm_gbs=d["hbm_gbs"], bf16_tflops=d["bf16_tflops"],
+                    bf16_tflops_sustained=d.get("bf16_tflops_sustained"), source="of measured")
+    return dict(hbm_gbs=6650.0, bf16_tflops=1590.0, bf16_tflops_sustained=1400.0, source="of fallback")
+
+
+def fp32_simt_peak_tflops(torch):
+    """FP32 CUDA-core GEMM throughput (cuBLAS SGEMM, TF32 off) as the FFMA
+    reference point for the float32 kernels."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, device="cuda")
+        b = torch.randn(n, n, device="cuda")
+        c = torch.empty(n, n, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b, out=c)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b, out=c)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b, c
+        return 2 * n**3 / (best * 1e-3) / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
+def ncu_traffic():
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
+def run_ours(args, wl):
+    import torch
+    import torch.distributed as dist
+
+    from lowrank_gpu_fastest_b200 import api
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    shape, patch, stride = wl["shape"], wl["patch"], wl["stride"]
+
+    # CPU baseline first (spawn pool before any heavy GPU work), rank 0 at N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        vol0, _ = make_phantom_lowrank(shape, seed=0)
+        cores = host_cores()
+        n = args.cpu_sample or max(64, 48 * cores)
+        rate, dt, used = cpu_step0_rate(vol0, patch, stride, n, cores)
+        cpu = dict(value=rate, unit="patches/s", cores=used, kind="port",
+                   sample=f"{n} patches evenly spaced over the corner list, step-0 NumPy loop "
+                          f"(SVD + MP rank + weighted accumulate), {used} spawn workers x 1 BLAS "
+                          f"thread, {dt:.1f} s wall")
+
+    vol, _ = make_phantom_lowrank(shape, seed=rank)
+    dev = torch.device("cuda", local)
+    d_vol = torch.from_numpy(vol).to(dev)
+    d_out = torch.empty_like(d_vol)
+    plan = api.get_plan(shape, patch, stride, form=args.form, device=local)
+    ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=dev)
+    d_ranks = torch.empty(plan.n_patches, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sid = stream.cuda_stream
+    P = plan.n_patches
+
+    def step():
+        plan.denoise(d_vol.data_ptr(), d_out.data_ptr(), d_ranks.data_ptr(), ws.data_ptr(), sid)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    plan.set_profiling(True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter()
+    for s, e in evs:
+        flush.zero_()
+        s.record(stream)
+        step()
+        e.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    phases, ncalls = plan.phase_ms()
+    plan.set_profiling(False)
+    ms_total = sum(s.elapsed_time(e) for s, e in evs)
+    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t.item()) / args.steps
+    value = world * P / (ms_per_step * 1e-3)
+
+    # e2e: host buffers through the C ABI (pinned in/out), copies inside the timed region
+    h_in = torch.from_numpy(vol).pin_memory()
+    h_out = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+    h_ranks = torch.empty(P, dtype=torch.int32, pin_memory=True)
+    d_in = torch.empty_like(d_vol)
+
+    def e2e_step():
+        plan.denoise_host(h_in.data_ptr(), h_out.data_ptr(), h_ranks.data_ptr(), d_in.data_ptr(),
+                          d_out.data_ptr(), d_ranks.data_ptr(), ws.data_ptr(), sid)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()  # returns after the D2H copies completed
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    t = torch.tensor([statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms_step = float(t.item())
+
+    if rank == 0:
+        vbytes = int(np.prod(shape)) * 4
+        peaks = measured_peaks()
+        ph = {k: v / max(ncalls, 1) for k, v in phases.items()}
+        dom = max(ph, key=ph.get)
+        N = int(np.prod(patch))
+        T = shape[3]
+        flops_unit = {"gram": 2 * N * T * T, "recon": 2 * N * T * T}
+        traffic = ncu_traffic().get(PHASE_KERNEL[dom])
+        if dom in flops_unit:
+            achieved = flops_unit[dom] * P / (ph[dom] * 1e-3) / 1e12
+            roof = dict(kernel=PHASE_KERNEL[dom], bound="tensor", achieved=achieved,
+                        peak=peaks["bf16_tflops"], unit="TFLOP/s",
+                        frac=achieved / peaks["bf16_tflops"], traffic=traffic,
+                        peak_source=f"bf16 dense burst {peaks['source']}",
+                        algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch")
+        else:
+            byts = {"center": 2 * vbytes + vbytes // T, "eigh_mp": 2 * P * T * T * 4}[dom]
+            achieved = byts / (ph[dom] * 1e-3) / 1e9
+            roof = dict(kernel=PHASE_KERNEL[dom], bound="hbm", achieved=achieved, peak=peaks["hbm_gbs"],
+                        unit="GB/s", frac=achieved / peaks["hbm_gbs"], traffic=traffic,
+                        peak_source=f"HBM copy {peaks['source']}")
+        fp32_peak = fp32_simt_peak_tflops(torch)
+        total_flops = 4 * N * T * T * P
+        line = dict(
+            metric="patches_per_s", value=value, unit="patches/s", n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=ms_per_step, ms_per_volume=ms_per_step,
+            higher_is_better=True, scaling="weak",
+            vs_baseline=(world * P / (e2e_ms_step * 1e-3)) / (12600 / (PUBLISHED_STEP8_MS * 1e-3))
+            if wl is WORKLOADS["headline"] else None,
+            vs_baseline_basis="e2e host->host patches/s / published step-8 (66.5 ms host->host, "
+                              "12600 patches, unstated GPU)",
+            dtype="f32", data="synthetic",
+            config=dict(workload=wl["desc"], shape=list(shape), patch=list(patch), stride=stride,
+                        form=args.form, phantom="rank-4 [0,1] + N(0,0.05^2), seed = rank",
+                        l2="flushed by a 256 MiB write between timed steps (outside the events)",
+                        parallelism=f"replica x{world}" if world > 1 else "single GPU"),
+            e2e=dict(value=world * P / (e2e_ms_step * 1e-3), unit="patches/s",
+                     ms_per_step=e2e_ms_step, h2d_bytes_per_step=vbytes,
+                     d2h_bytes_per_step=vbytes + 4 * P,
+                     path="lrd_denoise_host (pinned host in/out, H2D + denoise + D2H + sync)"),
+            phases_ms=ph,
+            roofline=roof,
+            fp32_simt=dict(peak_tflops_sgemm=fp32_peak,
+                           achieved_tflops_gram_recon=total_flops / ((ph["gram"] + ph["recon"]) * 1e-3) / 1e12),
+            cpu_baseline=cpu,
+            clocks=clocks,
+            gpu_launches=4 * args.steps if (plan.problem.batch == 0) else None,
+            wall_s_timed_region=wall,
+        )
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, wl)
+    else:
+        run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

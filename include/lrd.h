@@ -1,0 +1,131 @@
+/*
+ * lrd.h - C ABI of the B200 patch-wise MP-PCA denoiser (U-free Gram route).
+ *
+ * The ladder's drop-in call is the Python function ``denoise(vol_np) ->
+ * np.ndarray`` (step8_tuned.py:116-146, called by common.run, common.py:103,
+ * 130, 138) with patch shape, stride and batch taken from module globals
+ * (common.py:28-29, step8_tuned.py:21). This header is the native boundary
+ * under that call: plain pointers and sizes, device buffers owned by the
+ * caller, work enqueued on the caller's CUDA stream (passed as ``void*``), no
+ * host synchronisation inside ``lrd_denoise``.
+ *
+ * Conventions
+ *   - every function returns an int status: LRD_OK (0) or a negative LRD_ERR_*;
+ *     lrd_last_error_string() gives a message for the calling thread's last
+ *     failure;
+ *   - a volume is float32, C order (x, y, z, t), t contiguous;
+ *   - a plan is immutable after creation and may be shared between threads;
+ *     one stream must not run two calls on the same workspace at once.
+ */
+#ifndef LRD_H
+#define LRD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LRD_VERSION 1
+
+enum lrd_status {
+  LRD_OK = 0,
+  LRD_ERR_INVALID = -1,     /* bad argument, shape or null pointer          */
+  LRD_ERR_NOMEM = -2,       /* device allocation for the plan's tables failed */
+  LRD_ERR_CUDA = -3,        /* a CUDA call or launch failed                  */
+  LRD_ERR_UNSUPPORTED = -4, /* shape outside the compiled kernels' limits    */
+  LRD_ERR_NODEVICE = -5     /* no CUDA device / driver                       */
+};
+
+/* Arithmetic forms of the path. */
+enum lrd_form {
+  /* FP32 throughout; the weighted overlap accumulation runs per voxel in the
+   * ladder's patch order (x-major corners) with float32 rounding at every
+   * step, as step0_numpy_loop.py:36-39 does - deterministic. */
+  LRD_FORM_PLAIN = 0,
+  /* Same contractions; the accumulation keeps the temporal mean out of the
+   * running sums (out = m + sum w (x-m)P / sum w, float64 weight sums): error
+   * against a float64 run of the algorithm at the float32 output floor. */
+  LRD_FORM_ACCURATE = 1
+};
+
+/* One problem: volume (nx, ny, nz, nt), patch (px, py, pz), one stride for the
+ * three spatial axes (common.py:28-29, 37-44), the form, and ``batch`` = patches
+ * per Gram/eigensolver launch (step8_tuned.py:21; 0 = all in one launch). */
+typedef struct lrd_problem {
+  int32_t nx, ny, nz, nt;
+  int32_t px, py, pz;
+  int32_t stride;
+  int32_t form;
+  int32_t batch;
+} lrd_problem;
+
+typedef struct lrd_plan lrd_plan;
+
+/* Validate the problem, build the patch-index tables (common.py:37-44) on the
+ * current device, pick launch shapes. Replaces the per-call host work of
+ * step8_tuned.py:121-126 (allocation + patch_bases). */
+int lrd_plan_create(const lrd_problem* problem, lrd_plan** plan);
+int lrd_plan_destroy(lrd_plan* plan);
+
+/* Number of patches (common.py:37-44 product of the per-axis corner lists). */
+int lrd_plan_num_patches(const lrd_plan* plan, int64_t* n_patches);
+
+/* Bytes of device workspace ``lrd_denoise`` needs (temporal means, centred
+ * volume, per-patch Gram/eigenvector blocks, ranks, weights). Replaces the
+ * per-batch ``gram`` allocation of step8_tuned.py:130. */
+int lrd_workspace_size(const lrd_plan* plan, size_t* bytes);
+
+/* Denoise one volume, all on ``stream`` (a cudaStream_t; NULL = legacy
+ * default stream). ``d_vol`` and ``d_out`` are device arrays of
+ * nx*ny*nz*nt float32 and must not overlap; ``d_ranks`` (nullable) receives
+ * the MP rank chosen for every patch (int32, x-major patch order);
+ * ``d_workspace`` has ``lrd_workspace_size`` bytes, 256-byte aligned.
+ * Replaces step8_tuned.py:116-146 minus its host<->device copies: gather +
+ * Gram (gram_kernel, step8:32-56), eigh + MP rank + projector + weight
+ * (step8:134-137, mp_keep step8:96-113), reconstruction + weighted overlap
+ * add (recon_scatter_kernel, step8:59-86) and the normalisation (step8:145). */
+int lrd_denoise(const lrd_plan* plan, const float* d_vol, float* d_out, int32_t* d_ranks,
+                void* d_workspace, void* stream);
+
+/* Host-buffer form of lrd_denoise: copies ``h_vol`` (pinned or pageable host
+ * memory) to ``d_in``, denoises into ``d_out``, copies the result to
+ * ``h_out`` and waits for the stream. ``d_in``/``d_out`` are caller-owned
+ * device buffers of the volume's size. This is the whole host->host call of
+ * step8_tuned.py:116-146 (from_numpy().cuda() ... host.copy_(...)). */
+int lrd_denoise_host(const lrd_plan* plan, const float* h_vol, float* h_out, int32_t* h_ranks,
+                     float* d_in, float* d_out, int32_t* d_ranks, void* d_workspace,
+                     void* stream);
+
+/* Stage entry points, for per-stage parity checks against step 4's unfused
+ * route (step4_gram_eigh.py:60-67).
+ *   lrd_stage_gram: G = Xc^T Xc for every patch -> d_gram (n_patches, nt, nt).
+ *   lrd_stage_eigh: from d_gram, ascending eigenvalues -> d_lam (n_patches, nt)
+ *     (nullable), the top-p eigenvectors in descending eigenvalue order as a
+ *     compact row-major nt x p matrix at the start of each patch's nt*nt slot
+ *     of d_vecs, MP ranks -> d_ranks. d_gram is left unchanged. */
+int lrd_stage_gram(const lrd_plan* plan, const float* d_vol, float* d_gram, void* d_workspace,
+                   void* stream);
+int lrd_stage_eigh(const lrd_plan* plan, const float* d_gram, float* d_lam, float* d_vecs,
+                   int32_t* d_ranks, void* d_workspace, void* stream);
+
+/* Measurement hook (no counterpart in the reference): with profiling on,
+ * every lrd_denoise call records CUDA events between its phases on its
+ * stream; lrd_plan_phase_ms waits for the last recorded call and returns, per
+ * phase, the summed milliseconds and the number of calls recorded since the
+ * previous read (then clears them). Phases: 0 centring, 1 Gram, 2 eigensolver
+ * + MP rank, 3 reconstruction + accumulation. Profiling state is per plan and
+ * not thread-safe. */
+#define LRD_NUM_PHASES 4
+int lrd_plan_set_profiling(lrd_plan* plan, int enable);
+int lrd_plan_phase_ms(lrd_plan* plan, float* ms /* LRD_NUM_PHASES */, int32_t* n_calls);
+
+/* Message of the calling thread's last failure ("" if none). */
+const char* lrd_last_error_string(void);
+int lrd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LRD_H */

@@ -1,0 +1,24 @@
+"""B200-native patch-wise MP-PCA denoiser (U-free Gram route).
+
+Public surface:
+
+* :func:`denoise` - drop-in for the ladder's ``denoise`` entry point
+  (step8_tuned.py:116-146) with patch / stride / batch as arguments;
+* :mod:`.problem` - the patch index space (common.py:37-44);
+* :mod:`.harness` - phantoms and the ``common.run``-style timing harness;
+* :mod:`._native` - the ctypes binding of ``liblrd.so`` (include/lrd.h).
+"""
+
+from .problem import Problem, patch_corners, patch_bases, n_patches  # noqa: F401
+from .harness import make_phantom, make_phantom_lowrank, rel_l2  # noqa: F401
+
+
+def denoise(*args, **kwargs):
+    """See :func:`lowrank_gpu_fastest_b200.api.denoise`."""
+    from .api import denoise as _d
+
+    return _d(*args, **kwargs)
+
+
+__all__ = ["denoise", "Problem", "patch_corners", "patch_bases", "n_patches", "make_phantom",
+           "make_phantom_lowrank", "rel_l2"]

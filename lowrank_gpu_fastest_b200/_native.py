@@ -1,0 +1,143 @@
+"""ctypes binding of ``liblrd.so`` (declarations in include/lrd.h).
+
+The library is the only compute path: if it is missing or fails to load, every
+entry point raises - there is no CPU or PyTorch fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblrd.so")
+
+LRD_OK = 0
+LRD_ERR_INVALID = -1
+LRD_ERR_NOMEM = -2
+LRD_ERR_CUDA = -3
+LRD_ERR_UNSUPPORTED = -4
+LRD_ERR_NODEVICE = -5
+
+FORMS = {"plain": 0, "accurate": 1}
+
+# Every symbol include/lrd.h declares, with (restype, argtypes).
+_c_i32p = ctypes.POINTER(ctypes.c_int32)
+_c_f32p = ctypes.c_void_p
+SIGNATURES = {
+    "lrd_version": (ctypes.c_int, []),
+    "lrd_last_error_string": (ctypes.c_char_p, []),
+    "lrd_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "lrd_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "lrd_plan_num_patches": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]),
+    "lrd_workspace_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "lrd_denoise": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 5),
+    "lrd_denoise_host": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 8),
+    "lrd_stage_gram": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 4),
+    "lrd_stage_eigh": (ctypes.c_int, [ctypes.c_void_p] + [ctypes.c_void_p] * 6),
+    "lrd_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "lrd_plan_phase_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_int32)]),
+}
+PHASES = ("center", "gram", "eigh_mp", "recon")
+
+
+class LrdProblem(ctypes.Structure):
+    """``struct lrd_problem`` (include/lrd.h)."""
+
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("nx", "ny", "nz", "nt", "px", "py", "pz", "stride", "form", "batch")]
+
+
+class LrdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"lrd error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load(path: str | None = None):
+    """Load (once) and return the native library. Raises if it is absent."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise ImportError(
+                f"{p} not found: build it with `python -m lowrank_gpu_fastest_b200.build` "
+                "(the CUDA library is the only compute path)")
+        lib = ctypes.CDLL(p)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc: int):
+    if rc != LRD_OK:
+        msg = load().lrd_last_error_string().decode(errors="replace")
+        raise LrdError(rc, msg)
+
+
+class Plan:
+    """Owns an ``lrd_plan*`` for one problem on the current CUDA device."""
+
+    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0):
+        lib = load()
+        if form not in FORMS:
+            raise ValueError(f"form must be one of {sorted(FORMS)}, got {form!r}")
+        nx, ny, nz, nt = (int(s) for s in shape)
+        px, py, pz = (int(p) for p in patch)
+        self.problem = LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0))
+        self.shape = (nx, ny, nz, nt)
+        self.patch = (px, py, pz)
+        self.stride = int(stride)
+        self.form = form
+        h = ctypes.c_void_p()
+        check(lib.lrd_plan_create(ctypes.byref(self.problem), ctypes.byref(h)))
+        self.handle = h
+        n = ctypes.c_int64()
+        check(lib.lrd_plan_num_patches(h, ctypes.byref(n)))
+        self.n_patches = int(n.value)
+        ws = ctypes.c_size_t()
+        check(lib.lrd_workspace_size(h, ctypes.byref(ws)))
+        self.workspace_bytes = int(ws.value)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                load().lrd_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    def denoise(self, d_vol: int, d_out: int, d_ranks: int | None, d_ws: int, stream: int):
+        check(load().lrd_denoise(self.handle, d_vol, d_out, d_ranks, d_ws, stream))
+
+    def denoise_host(self, h_vol, h_out, h_ranks, d_in, d_out, d_ranks, d_ws, stream):
+        check(load().lrd_denoise_host(self.handle, h_vol, h_out, h_ranks, d_in, d_out, d_ranks, d_ws,
+                                      stream))
+
+    def set_profiling(self, enable: bool):
+        check(load().lrd_plan_set_profiling(self.handle, int(bool(enable))))
+
+    def phase_ms(self):
+        """Summed ms per phase and call count since the last read (clears)."""
+        ms = (ctypes.c_float * len(PHASES))()
+        n = ctypes.c_int32()
+        check(load().lrd_plan_phase_ms(self.handle, ms, ctypes.byref(n)))
+        return dict(zip(PHASES, list(ms))), int(n.value)
+
+    def stage_gram(self, d_vol, d_gram, d_ws, stream):
+        check(load().lrd_stage_gram(self.handle, d_vol, d_gram, d_ws, stream))
+
+    def stage_eigh(self, d_gram, d_lam, d_vecs, d_ranks, d_ws, stream):
+        check(load().lrd_stage_eigh(self.handle, d_gram, d_lam, d_vecs, d_ranks, d_ws, stream))

@@ -1,0 +1,514 @@
+// C ABI of the MP-PCA denoiser: plans, workspace, launches (include/lrd.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lrd.h"
+#include "center.cuh"
+#include "eigh.cuh"
+#include "gram.cuh"
+#include "lrd_common.cuh"
+#include "recon.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+  return fail(LRD_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(err), cudaGetErrorName(err));
+}
+
+#define LRD_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Sorted corner positions along one axis (common.py:40-43):
+// sorted({*range(0, s - p + 1, step), s - p}).
+std::vector<int32_t> axis_corners(int size, int patch, int stride) {
+  std::vector<int32_t> c;
+  for (int v = 0; v <= size - patch; v += stride) c.push_back(v);
+  if (c.empty() || c.back() != size - patch) c.push_back(size - patch);
+  return c;
+}
+
+}  // namespace
+
+struct lrd_plan {
+  lrd_problem prob;
+  lrd::Geom g;
+  int device;
+  long long nvox;
+  int tpt;                 // recon frames per thread
+  int gram_threads;
+  size_t smem_center, smem_gram, smem_eigh, smem_recon;
+  int center_warps;
+  // workspace offsets (bytes)
+  size_t off_mean, off_xc, off_gv, off_rank, off_wgt, ws_bytes;
+  // device tables (one allocation)
+  void* d_tables;
+  lrd::AxisTables tab;
+  // measurement hook: a ring of per-call phase events
+  bool profiling = false;
+  int prof_calls = 0;
+  std::vector<cudaEvent_t> prof_events;  // kProfRing * (LRD_NUM_PHASES + 1)
+};
+
+namespace {
+constexpr int kProfRing = 256;
+}
+
+namespace {
+
+constexpr int kTptChoices[] = {4, 6, 8, 12, 16, 24, 32};
+
+int pick_tpt(int T) {
+  const int need = (T + lrd::kReconSplit - 1) / lrd::kReconSplit;
+  for (int c : kTptChoices)
+    if (c >= need) return c;
+  return -1;
+}
+
+// Brick choice for the reconstruction: minimise the thread-slots the CTAs spend
+// on (voxel, touching patch) pairs, per axis sum_b touch(b) * b, with 64..512
+// threads per CTA.
+struct BrickAxis {
+  long long slots;
+  int nblocks;
+};
+
+BrickAxis brick_axis_cost(int size, int patch, const std::vector<int32_t>& corners, int bsz) {
+  BrickAxis r{0, (size + bsz - 1) / bsz};
+  for (int b = 0; b < r.nblocks; ++b) {
+    const int lo = b * bsz, hi = std::min(size, lo + bsz) - 1;
+    int touch = 0;
+    for (int32_t c : corners)
+      if (c <= hi && c + patch - 1 >= lo) ++touch;
+    r.slots += (long long)touch * bsz;
+  }
+  return r;
+}
+
+template <int TPT>
+void* recon_fn(bool accurate) {
+  return accurate ? (void*)lrd::recon_kernel<TPT, true> : (void*)lrd::recon_kernel<TPT, false>;
+}
+
+void* recon_kernel_ptr(int tpt, bool accurate) {
+  switch (tpt) {
+    case 4: return recon_fn<4>(accurate);
+    case 6: return recon_fn<6>(accurate);
+    case 8: return recon_fn<8>(accurate);
+    case 12: return recon_fn<12>(accurate);
+    case 16: return recon_fn<16>(accurate);
+    case 24: return recon_fn<24>(accurate);
+    case 32: return recon_fn<32>(accurate);
+  }
+  return nullptr;
+}
+
+int set_smem(const void* fn, size_t bytes) {
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(max dynamic smem)");
+  }
+  return LRD_OK;
+}
+
+int launch_check(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  return LRD_OK;
+}
+
+int run_center(const lrd_plan* P, const float* d_vol, char* ws, cudaStream_t st) {
+  float* mean = reinterpret_cast<float*>(ws + P->off_mean);
+  float* xc = reinterpret_cast<float*>(ws + P->off_xc);
+  const long long per_block = 32LL * P->center_warps;
+  const long long blocks = (P->nvox + per_block - 1) / per_block;
+  lrd::center_kernel<<<(unsigned)blocks, 32 * P->center_warps, P->smem_center, st>>>(
+      d_vol, xc, mean, P->nvox, P->g.nt);
+  return launch_check("center_kernel launch");
+}
+
+int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
+  const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
+  const long long npatch = P->g.npatch;
+  const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
+  const long long TT = (long long)P->g.nt * P->g.nt;
+  for (long long p0 = 0; p0 < npatch; p0 += batch) {
+    const long long nb = std::min(batch, npatch - p0);
+    lrd::gram_kernel<<<(unsigned)nb, P->gram_threads, P->smem_gram, st>>>(xc, d_gram + p0 * TT, P->g,
+                                                                         P->tab, p0);
+    int rc = launch_check("gram_kernel launch");
+    if (rc) return rc;
+  }
+  return LRD_OK;
+}
+
+int run_eigh(const lrd_plan* P, const float* d_gram, float* d_vecs, float* d_lam, int32_t* d_rank,
+             float* d_wgt, cudaStream_t st) {
+  const long long npatch = P->g.npatch;
+  const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
+  const int T = P->g.nt;
+  const long long TT = (long long)T * T;
+  for (long long p0 = 0; p0 < npatch; p0 += batch) {
+    const long long nb = std::min(batch, npatch - p0);
+    lrd::eigh_mp_kernel<<<(unsigned)nb, 32, P->smem_eigh, st>>>(
+        d_gram + p0 * TT, d_vecs + p0 * TT, d_lam ? d_lam + p0 * T : nullptr, d_rank + p0, d_wgt + p0,
+        T, P->g.nvox_patch);
+    int rc = launch_check("eigh_mp_kernel launch");
+    if (rc) return rc;
+  }
+  return LRD_OK;
+}
+
+int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st) {
+  const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
+  const float* mean = reinterpret_cast<const float*>(ws + P->off_mean);
+  const float* gv = reinterpret_cast<const float*>(ws + P->off_gv);
+  const int32_t* rank = reinterpret_cast<const int32_t*>(ws + P->off_rank);
+  const float* wgt = reinterpret_cast<const float*>(ws + P->off_wgt);
+  const bool acc = P->prob.form == LRD_FORM_ACCURATE;
+  const unsigned nbricks = (unsigned)((long long)P->g.nbx * P->g.nby * P->g.nbz);
+  const unsigned threads = (unsigned)(P->g.bx * P->g.by * P->g.bz * lrd::kReconSplit);
+  void* fn = recon_kernel_ptr(P->tpt, acc);
+  lrd::Geom g = P->g;
+  lrd::AxisTables tab = P->tab;
+  void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv, (void*)&rank, (void*)&wgt,
+                  (void*)&d_out, (void*)&g, (void*)&tab};
+  cudaError_t e = cudaLaunchKernel(fn, dim3(nbricks), dim3(threads), args, P->smem_recon, st);
+  if (e != cudaSuccess) return cuda_fail(e, "recon_kernel launch");
+  return LRD_OK;
+}
+
+int check_plan(const lrd_plan* P) {
+  if (!P) return fail(LRD_ERR_INVALID, "plan is NULL");
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev != P->device)
+    return fail(LRD_ERR_INVALID, "plan was created on device %d but device %d is current", P->device, dev);
+  return LRD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrd_version(void) { return LRD_VERSION; }
+
+const char* lrd_last_error_string(void) { return g_last_error.c_str(); }
+
+int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
+  g_last_error.clear();
+  if (!pr || !out) return fail(LRD_ERR_INVALID, "problem or plan pointer is NULL");
+  *out = nullptr;
+  const int dims[3] = {pr->nx, pr->ny, pr->nz};
+  const int pat[3] = {pr->px, pr->py, pr->pz};
+  for (int a = 0; a < 3; ++a) {
+    if (dims[a] < 1) return fail(LRD_ERR_INVALID, "volume axis %d has size %d", a, dims[a]);
+    if (pat[a] < 1 || pat[a] > dims[a])
+      return fail(LRD_ERR_INVALID, "patch side %d (axis %d) must be in [1, %d]", pat[a], a, dims[a]);
+  }
+  if (pr->nt < 2) return fail(LRD_ERR_INVALID, "need at least 2 frames, got %d", pr->nt);
+  if (pr->nt > lrd::kMaxT) return fail(LRD_ERR_UNSUPPORTED, "nt=%d exceeds the compiled limit %d", pr->nt, lrd::kMaxT);
+  if (pr->stride < 1) return fail(LRD_ERR_INVALID, "stride must be >= 1, got %d", pr->stride);
+  if (pr->form != LRD_FORM_PLAIN && pr->form != LRD_FORM_ACCURATE)
+    return fail(LRD_ERR_INVALID, "unknown form %d", pr->form);
+  if (pr->batch < 0) return fail(LRD_ERR_INVALID, "batch must be >= 0, got %d", pr->batch);
+  const long long nvox = (long long)pr->nx * pr->ny * pr->nz;
+  if (nvox * pr->nt >= (1LL << 40)) return fail(LRD_ERR_UNSUPPORTED, "volume too large");
+  const long long nvp = (long long)pr->px * pr->py * pr->pz;
+  if (nvp > (1 << 30)) return fail(LRD_ERR_UNSUPPORTED, "patch too large");
+  if (nvp < pr->nt)
+    return fail(LRD_ERR_UNSUPPORTED,
+                "patch has %lld voxels < %d frames: the Gram route needs N >= T", nvp, pr->nt);
+
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(LRD_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+
+  std::vector<int32_t> corners[3], cover[3], brick[3];
+  for (int a = 0; a < 3; ++a) {
+    corners[a] = axis_corners(dims[a], pat[a], pr->stride);
+    cover[a].resize(2 * (size_t)dims[a]);
+    for (int x = 0; x < dims[a]; ++x) {
+      int lo = -1, hi = -2;
+      for (int i = 0; i < (int)corners[a].size(); ++i) {
+        const int c = corners[a][i];
+        if (c <= x && x <= c + pat[a] - 1) {
+          if (lo < 0) lo = i;
+          hi = i;
+        }
+      }
+      cover[a][2 * x] = lo;
+      cover[a][2 * x + 1] = hi;
+    }
+  }
+  // brick shape
+  int best[3] = {1, 1, 1};
+  double best_cost = 1e300;
+  for (int bx = 1; bx <= 16; ++bx)
+    for (int by = 1; by <= 16; ++by)
+      for (int bz = 1; bz <= 32; ++bz) {
+        const int threads = bx * by * bz * lrd::kReconSplit;
+        if (threads < 64 || threads > 512) continue;
+        if (bx > dims[0] + 0 && bx > 1) continue;
+        if (by > dims[1] && by > 1) continue;
+        if (bz > dims[2] && bz > 1) continue;
+        const BrickAxis ax = brick_axis_cost(dims[0], pat[0], corners[0], bx);
+        const BrickAxis ay = brick_axis_cost(dims[1], pat[1], corners[1], by);
+        const BrickAxis az = brick_axis_cost(dims[2], pat[2], corners[2], bz);
+        const long long nbr = (long long)ax.nblocks * ay.nblocks * az.nblocks;
+        // slots plus a per-(brick, patch) fixed cost (barriers, V staging)
+        const double touch = (double)ax.slots / bx * ay.slots / by * az.slots / bz;  // sum over bricks of touching patches
+        const double cost = (double)ax.slots * ay.slots * az.slots + touch * 64.0 +
+                            (nbr < 296 ? 1e18 / (double)nbr : 0.0);
+        if (cost < best_cost) {
+          best_cost = cost;
+          best[0] = bx;
+          best[1] = by;
+          best[2] = bz;
+        }
+      }
+  const int bsz[3] = {best[0], best[1], best[2]};
+  for (int a = 0; a < 3; ++a) {
+    const int nb = (dims[a] + bsz[a] - 1) / bsz[a];
+    brick[a].resize(2 * (size_t)nb);
+    for (int b = 0; b < nb; ++b) {
+      const int lo = b * bsz[a], hi = std::min(dims[a], lo + bsz[a]) - 1;
+      int ilo = -1, ihi = -2;
+      for (int i = 0; i < (int)corners[a].size(); ++i) {
+        const int c = corners[a][i];
+        if (c <= hi && c + pat[a] - 1 >= lo) {
+          if (ilo < 0) ilo = i;
+          ihi = i;
+        }
+      }
+      brick[a][2 * b] = ilo;
+      brick[a][2 * b + 1] = ihi;
+    }
+  }
+
+  lrd_plan* P = new lrd_plan();
+  P->prob = *pr;
+  P->device = dev;
+  P->nvox = nvox;
+  lrd::Geom& g = P->g;
+  g.nx = pr->nx; g.ny = pr->ny; g.nz = pr->nz; g.nt = pr->nt;
+  g.px = pr->px; g.py = pr->py; g.pz = pr->pz;
+  g.ncx = (int)corners[0].size(); g.ncy = (int)corners[1].size(); g.ncz = (int)corners[2].size();
+  g.npatch = (long long)g.ncx * g.ncy * g.ncz;
+  g.nvox_patch = (int)nvp;
+  g.bx = bsz[0]; g.by = bsz[1]; g.bz = bsz[2];
+  g.nbx = (int)brick[0].size() / 2; g.nby = (int)brick[1].size() / 2; g.nbz = (int)brick[2].size() / 2;
+
+  // device tables
+  size_t total = 0;
+  size_t offs[9];
+  const std::vector<int32_t>* tabs[9] = {&corners[0], &corners[1], &corners[2], &cover[0], &cover[1],
+                                         &cover[2],   &brick[0],   &brick[1],   &brick[2]};
+  for (int i = 0; i < 9; ++i) {
+    offs[i] = total;
+    total += align256(tabs[i]->size() * sizeof(int32_t));
+  }
+  std::vector<char> host(total, 0);
+  for (int i = 0; i < 9; ++i) memcpy(host.data() + offs[i], tabs[i]->data(), tabs[i]->size() * sizeof(int32_t));
+  e = cudaMalloc(&P->d_tables, total);
+  if (e != cudaSuccess) {
+    delete P;
+    return fail(LRD_ERR_NOMEM, "cudaMalloc(%zu) for plan tables: %s", total, cudaGetErrorString(e));
+  }
+  e = cudaMemcpy(P->d_tables, host.data(), total, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(P->d_tables);
+    delete P;
+    return cuda_fail(e, "cudaMemcpy plan tables");
+  }
+  char* base = static_cast<char*>(P->d_tables);
+  for (int a = 0; a < 3; ++a) {
+    P->tab.corners[a] = reinterpret_cast<const int32_t*>(base + offs[a]);
+    P->tab.cover[a] = reinterpret_cast<const int32_t*>(base + offs[3 + a]);
+    P->tab.brick[a] = reinterpret_cast<const int32_t*>(base + offs[6 + a]);
+  }
+
+  const int T = pr->nt;
+  P->tpt = pick_tpt(T);
+  const int nb4 = (T + 3) / 4;
+  P->gram_threads = nb4 * (nb4 + 1) / 2;
+  P->center_warps = 4;
+  P->smem_center = sizeof(float) * (size_t)P->center_warps * (32 * (T + 1) + 32);
+  P->smem_gram = sizeof(float) * (size_t)pr->py * pr->pz * (4 * nb4);
+  P->smem_eigh = sizeof(float) * lrd::eigh_smem_floats(T);
+  P->smem_recon = sizeof(float) * (size_t)T * (T | 1);
+  int rc = set_smem((const void*)lrd::center_kernel, P->smem_center);
+  if (!rc) rc = set_smem((const void*)lrd::gram_kernel, P->smem_gram);
+  if (!rc) rc = set_smem((const void*)lrd::eigh_mp_kernel, P->smem_eigh);
+  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, false), P->smem_recon);
+  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, true), P->smem_recon);
+  if (rc) {
+    cudaFree(P->d_tables);
+    delete P;
+    return rc;
+  }
+  if (P->smem_gram > 227 * 1024 || P->smem_eigh > 227 * 1024) {
+    cudaFree(P->d_tables);
+    delete P;
+    return fail(LRD_ERR_UNSUPPORTED, "patch plane or T too large for shared memory");
+  }
+
+  // workspace layout
+  size_t off = 0;
+  P->off_mean = off; off += align256(sizeof(float) * (size_t)nvox);
+  P->off_xc = off; off += align256(sizeof(float) * (size_t)nvox * T);
+  P->off_gv = off; off += align256(sizeof(float) * (size_t)g.npatch * T * T);
+  P->off_rank = off; off += align256(sizeof(int32_t) * (size_t)g.npatch);
+  P->off_wgt = off; off += align256(sizeof(float) * (size_t)g.npatch);
+  P->ws_bytes = off;
+  *out = P;
+  return LRD_OK;
+}
+
+int lrd_plan_set_profiling(lrd_plan* P, int enable) {
+  if (!P) return fail(LRD_ERR_INVALID, "plan is NULL");
+  if (enable && P->prof_events.empty()) {
+    P->prof_events.resize((size_t)kProfRing * (LRD_NUM_PHASES + 1));
+    for (auto& e : P->prof_events) LRD_CUDA(cudaEventCreate(&e));
+  }
+  P->profiling = enable != 0;
+  P->prof_calls = 0;
+  return LRD_OK;
+}
+
+int lrd_plan_phase_ms(lrd_plan* P, float* ms, int32_t* n_calls) {
+  if (!P || !ms) return fail(LRD_ERR_INVALID, "NULL argument");
+  for (int k = 0; k < LRD_NUM_PHASES; ++k) ms[k] = 0.f;
+  const int n = P->prof_calls;
+  if (n > 0) {
+    const cudaEvent_t* ev = P->prof_events.data();
+    LRD_CUDA(cudaEventSynchronize(ev[(size_t)(n - 1) * (LRD_NUM_PHASES + 1) + LRD_NUM_PHASES]));
+    for (int c = 0; c < n; ++c)
+      for (int k = 0; k < LRD_NUM_PHASES; ++k) {
+        float t = 0.f;
+        LRD_CUDA(cudaEventElapsedTime(&t, ev[(size_t)c * (LRD_NUM_PHASES + 1) + k],
+                                      ev[(size_t)c * (LRD_NUM_PHASES + 1) + k + 1]));
+        ms[k] += t;
+      }
+  }
+  if (n_calls) *n_calls = n;
+  P->prof_calls = 0;
+  return LRD_OK;
+}
+
+int lrd_plan_destroy(lrd_plan* P) {
+  if (!P) return LRD_OK;
+  for (auto& e : P->prof_events) cudaEventDestroy(e);
+  if (P->d_tables) cudaFree(P->d_tables);
+  delete P;
+  return LRD_OK;
+}
+
+int lrd_plan_num_patches(const lrd_plan* P, int64_t* n) {
+  if (!P || !n) return fail(LRD_ERR_INVALID, "NULL argument");
+  *n = P->g.npatch;
+  return LRD_OK;
+}
+
+int lrd_workspace_size(const lrd_plan* P, size_t* bytes) {
+  if (!P || !bytes) return fail(LRD_ERR_INVALID, "NULL argument");
+  *bytes = P->ws_bytes;
+  return LRD_OK;
+}
+
+int lrd_denoise(const lrd_plan* P, const float* d_vol, float* d_out, int32_t* d_ranks, void* d_ws,
+                void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!d_vol || !d_out || !d_ws) return fail(LRD_ERR_INVALID, "NULL device buffer");
+  if (reinterpret_cast<uintptr_t>(d_ws) % 256) return fail(LRD_ERR_INVALID, "workspace not 256-byte aligned");
+  const size_t vbytes = sizeof(float) * (size_t)P->nvox * P->g.nt;
+  const char* a = reinterpret_cast<const char*>(d_vol);
+  const char* b = reinterpret_cast<const char*>(d_out);
+  if (a < b + vbytes && b < a + vbytes) return fail(LRD_ERR_INVALID, "d_vol and d_out overlap");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(d_ws);
+  float* gv = reinterpret_cast<float*>(ws + P->off_gv);
+  int32_t* rank = reinterpret_cast<int32_t*>(ws + P->off_rank);
+  float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
+  cudaEvent_t* ev = nullptr;
+  if (P->profiling && P->prof_calls < kProfRing) {
+    ev = const_cast<cudaEvent_t*>(P->prof_events.data()) + (size_t)P->prof_calls * (LRD_NUM_PHASES + 1);
+    ++const_cast<lrd_plan*>(P)->prof_calls;
+  }
+  if (ev) LRD_CUDA(cudaEventRecord(ev[0], st));
+  if ((rc = run_center(P, d_vol, ws, st))) return rc;
+  if (ev) LRD_CUDA(cudaEventRecord(ev[1], st));
+  if ((rc = run_gram(P, ws, gv, st))) return rc;
+  if (ev) LRD_CUDA(cudaEventRecord(ev[2], st));
+  if ((rc = run_eigh(P, gv, gv, nullptr, rank, wgt, st))) return rc;
+  if (ev) LRD_CUDA(cudaEventRecord(ev[3], st));
+  if ((rc = run_recon(P, ws, d_out, st))) return rc;
+  if (ev) LRD_CUDA(cudaEventRecord(ev[4], st));
+  if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToDevice, st));
+  return LRD_OK;
+}
+
+int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_t* h_ranks, float* d_in,
+                     float* d_out, int32_t* d_ranks, void* d_ws, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!h_vol || !h_out || !d_in || !d_out) return fail(LRD_ERR_INVALID, "NULL buffer");
+  if (h_ranks && !d_ranks) return fail(LRD_ERR_INVALID, "h_ranks needs d_ranks");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t vbytes = sizeof(float) * (size_t)P->nvox * P->g.nt;
+  LRD_CUDA(cudaMemcpyAsync(d_in, h_vol, vbytes, cudaMemcpyHostToDevice, st));
+  if ((rc = lrd_denoise(P, d_in, d_out, d_ranks, d_ws, stream))) return rc;
+  LRD_CUDA(cudaMemcpyAsync(h_out, d_out, vbytes, cudaMemcpyDeviceToHost, st));
+  if (h_ranks)
+    LRD_CUDA(cudaMemcpyAsync(h_ranks, d_ranks, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToHost, st));
+  LRD_CUDA(cudaStreamSynchronize(st));
+  return LRD_OK;
+}
+
+int lrd_stage_gram(const lrd_plan* P, const float* d_vol, float* d_gram, void* d_ws, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!d_vol || !d_gram || !d_ws) return fail(LRD_ERR_INVALID, "NULL device buffer");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(d_ws);
+  if ((rc = run_center(P, d_vol, ws, st))) return rc;
+  return run_gram(P, ws, d_gram, st);
+}
+
+int lrd_stage_eigh(const lrd_plan* P, const float* d_gram, float* d_lam, float* d_vecs, int32_t* d_ranks,
+                   void* d_ws, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!d_gram || !d_vecs || !d_ranks || !d_ws) return fail(LRD_ERR_INVALID, "NULL device buffer");
+  if (d_gram == d_vecs) return fail(LRD_ERR_INVALID, "d_gram and d_vecs must differ");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(d_ws);
+  float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
+  return run_eigh(P, d_gram, d_vecs, d_lam, d_ranks, wgt, st);
+}
+
+}  // extern "C"

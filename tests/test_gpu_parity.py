@@ -1,0 +1,157 @@
+"""Parity of the CUDA path (through the C ABI) with the step-0 oracle.
+
+Bars: MP ranks bit-exact; plain form within 2e-7 relative L2 of the
+reference's step-0 output; accurate form within 2e-7 (target 1e-7) of the
+float64 run of the algorithm.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import LARGE_CASES, SMALL_CASES, golden_input, load_golden
+from lowrank_gpu_fastest_b200 import _native, api, rel_l2
+from oracle import mppca as orc
+
+pytestmark = pytest.mark.gpu
+
+PLAIN_TOL = 2e-7          # relative L2 vs step 0 (plain form)
+ACCURATE_TOL = 2e-7       # relative L2 vs the float64 oracle (accurate form)
+ACCURATE_TOL_LARGE = 1e-7  # measured ~5e-8 at the 96x96x48x48 headline
+
+
+def run_dev(vol, patch, stride, form="plain", batch=None):
+    d = torch.from_numpy(vol).cuda()
+    out, ranks = api.denoise(d, patch, stride, batch, form=form, return_ranks=True)
+    torch.cuda.synchronize()
+    return out.cpu().numpy(), ranks.cpu().numpy()
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_small_plain_vs_step0(cuda_ok, name):
+    g = load_golden(name)
+    vol = golden_input(g)
+    out, ranks = run_dev(vol, tuple(g["patch"]), int(g["stride"]))
+    np.testing.assert_array_equal(ranks, g["ranks"])
+    assert rel_l2(out, g["out"]) <= PLAIN_TOL
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_small_accurate_vs_fp64(cuda_ok, name):
+    g = load_golden(name)
+    vol = golden_input(g)
+    out, ranks = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form="accurate")
+    np.testing.assert_array_equal(ranks, g["ranks"])
+    idx = g["sample_idx"]
+    assert rel_l2(out.reshape(-1)[idx], g["out64_sample"]) <= ACCURATE_TOL
+
+
+@pytest.mark.parametrize("name", LARGE_CASES)
+def test_large_ranks_and_sample(cuda_ok, name):
+    g = load_golden(name)
+    vol = golden_input(g)
+    out, ranks = run_dev(vol, tuple(g["patch"]), int(g["stride"]))
+    np.testing.assert_array_equal(ranks, g["ranks"])
+    idx = g["sample_idx"]
+    assert rel_l2(out.reshape(-1)[idx], g["out_sample"]) <= PLAIN_TOL
+    outa, _ = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form="accurate")
+    assert rel_l2(outa.reshape(-1)[idx], g["out64_sample"]) <= ACCURATE_TOL_LARGE
+
+
+def test_config1_full_volume_vs_live_oracle(cuda_ok):
+    g = load_golden("config1_lowrank")
+    vol = golden_input(g)
+    ref, ref_ranks = orc.denoise(vol, (11, 11, 11), 3)
+    out, ranks = run_dev(vol, (11, 11, 11), 3)
+    np.testing.assert_array_equal(ranks, ref_ranks)
+    assert rel_l2(out, ref) <= PLAIN_TOL
+
+
+def test_headline_region_vs_region_oracle(cuda_ok):
+    """A 9x9x9 box of the 96x96x48x48 volume against the step-0 loop run over
+    exactly the patches touching the box (bit-for-bit the full loop there)."""
+    g = load_golden("headline_ref")
+    vol = golden_input(g)
+    out, _ = run_dev(vol, (11, 11, 11), 3)
+    lo, hi = (40, 17, 20), (49, 26, 29)
+    box, _, _ = orc.denoise_region(vol, (11, 11, 11), 3, lo, hi)
+    assert rel_l2(out[40:49, 17:26, 20:29], box) <= PLAIN_TOL
+
+
+def test_deterministic_and_batch_invariant(cuda_ok):
+    g = load_golden("lowrank_p5s2")
+    vol = golden_input(g)
+    a, ra = run_dev(vol, (5, 5, 5), 2)
+    b, rb = run_dev(vol, (5, 5, 5), 2)
+    c, rc = run_dev(vol, (5, 5, 5), 2, batch=7)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
+    np.testing.assert_array_equal(ra, rc)
+
+
+def test_host_api_matches_device_api(cuda_ok):
+    g = load_golden("ref_small")
+    vol = golden_input(g)
+    host = api.denoise(vol, (11, 11, 11), 3)
+    assert isinstance(host, np.ndarray)
+    dev, _ = run_dev(vol, (11, 11, 11), 3)
+    np.testing.assert_array_equal(host, dev)
+
+
+def test_constant_volume_is_fixed_point(cuda_ok):
+    vol = np.full((9, 8, 10, 20), 2.5, dtype=np.float32)
+    out, ranks = run_dev(vol, (5, 5, 5), 2)
+    assert (ranks == 0).all()
+    ref, _ = orc.denoise(vol, (5, 5, 5), 2)
+    np.testing.assert_array_equal(out, ref)
+
+
+def test_uncovered_voxels_follow_ladder(cuda_ok):
+    """stride > patch side leaves voxels no patch covers: 0 / max(0, 1e-12) = 0."""
+    rng = np.random.default_rng(3)
+    vol = (rng.standard_normal((14, 12, 13, 24)) + 5).astype(np.float32)
+    ref, rref = orc.denoise(vol, (5, 5, 5), 7)
+    out, ranks = run_dev(vol, (5, 5, 5), 7)
+    np.testing.assert_array_equal(ranks, rref)
+    assert rel_l2(out, ref) <= PLAIN_TOL
+    outa, _ = run_dev(vol, (5, 5, 5), 7, form="accurate")
+    np.testing.assert_array_equal(outa[5:7], 0.0)
+
+
+def test_stage_gram_and_eigh_vs_fp64_oracle(cuda_ok):
+    g = load_golden("lowrank_p5s2")
+    vol = golden_input(g)
+    shape, patch, stride = vol.shape, (5, 5, 5), 2
+    plan = api.get_plan(shape, patch, stride)
+    T, P = shape[3], plan.n_patches
+    d = torch.from_numpy(vol).cuda()
+    ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device="cuda")
+    gram = torch.empty(P, T, T, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    plan.stage_gram(d.data_ptr(), gram.data_ptr(), ws.data_ptr(), s)
+    lam = torch.empty(P, T, device="cuda")
+    vecs = torch.zeros(P, T, T, device="cuda")
+    ranks = torch.empty(P, dtype=torch.int32, device="cuda")
+    plan.stage_eigh(gram.data_ptr(), lam.data_ptr(), vecs.data_ptr(), ranks.data_ptr(), ws.data_ptr(), s)
+    torch.cuda.synchronize()
+    gram, lam, vecs, ranks = (t.cpu().numpy() for t in (gram, lam, vecs, ranks))
+    corners = orc.patch_corners(shape, patch, stride)
+    for idx in range(0, P, 13):
+        i, j, k = corners[idx]
+        x = vol[i:i + 5, j:j + 5, k:k + 5].reshape(-1, T)
+        st = orc.gram_route_patch(x)
+        gscale = np.abs(st["G"]).max()
+        assert np.abs(gram[idx] - st["G"]).max() <= 1e-5 * gscale
+        # eigenvalues of our own Gram, to float32 round-off of its norm
+        lam_ref = np.linalg.eigvalsh(gram[idx].astype(np.float64))
+        assert np.abs(lam[idx] - lam_ref).max() <= 1e-5 * np.abs(lam_ref).max()
+        p = int(ranks[idx])
+        assert p == st["p"]
+        V = vecs[idx].reshape(-1)[: T * p].reshape(T, p).astype(np.float64)
+        np.testing.assert_allclose(V.T @ V, np.eye(p), atol=1e-5)
+        assert np.abs(V @ V.T - st["P"]).max() <= 1e-4
+
+
+def test_error_is_raised_for_bad_shapes(cuda_ok):
+    with pytest.raises(_native.LrdError):
+        api.denoise(torch.zeros(4, 4, 4, 8, device="cuda"), (5, 5, 5), 2)
