@@ -121,6 +121,32 @@ int lrd_stage_eigh(const lrd_plan* plan, const float* d_gram, float* d_lam, floa
 int lrd_plan_set_profiling(lrd_plan* plan, int enable);
 int lrd_plan_phase_ms(lrd_plan* plan, float* ms /* LRD_NUM_PHASES */, int32_t* n_calls);
 
+/* Denoise with no device allocation at all. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc (code running where the CUDA
+ * allocator is off limits, or a host framework that owns every device
+ * allocation): lrd_denoise needs a plan (whose index tables are
+ * cudaMalloc'd) and a caller-allocated workspace; this entry point needs
+ * neither. The caller passes only the problem, the input and output volumes
+ * and the optional rank array, all as for lrd_denoise. Every scratch buffer
+ * (patch-index tables, temporal means, centred volume, Gram/eigenvector
+ * blocks, ranks, weights) lives in one file-scope static device array of
+ * LRD_STATIC_SCRATCH_BYTES, which every GPU that loads the library holds
+ * until the process exits. Problems needing more scratch than that (about
+ * 21 MiB for a 48x48x24x48 volume with 11^3 patches at stride 3; the
+ * 96x96x48x48 headline needs about 203 MiB) are rejected with
+ * LRD_ERR_UNSUPPORTED and a message giving the size needed.
+ *
+ * The first call on a device looks up the array's device address (with that
+ * device current) and caches it; make that first call before any stream
+ * capture. All calls share the one array and it keeps the last call's
+ * contents (nothing in it needs to start at zero): calls whose work overlaps
+ * on the GPU - on different streams, or from different threads - race on it
+ * and must be serialised by the caller. */
+#define LRD_STATIC_SCRATCH_BYTES (32u << 20)
+int lrd_denoise_static(const lrd_problem* problem, const float* d_vol, float* d_out, int32_t* d_ranks,
+                       void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* lrd_last_error_string(void);
 int lrd_version(void);

@@ -39,6 +39,7 @@ SIGNATURES = {
     "lrd_plan_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "lrd_plan_phase_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int32)]),
+    "lrd_denoise_static": (ctypes.c_int, [ctypes.c_void_p] * 5),
 }
 PHASES = ("center", "gram", "eigh_mp", "recon")
 

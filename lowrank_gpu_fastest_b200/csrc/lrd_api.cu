@@ -512,3 +512,5 @@ int lrd_stage_eigh(const lrd_plan* P, const float* d_gram, float* d_lam, float* 
 }
 
 }  // extern "C"
+
+#include "lrd_static.inc"
