@@ -35,8 +35,12 @@ enum lrd_status {
   LRD_ERR_NOMEM = -2,       /* device allocation for the plan's tables failed */
   LRD_ERR_CUDA = -3,        /* a CUDA call or launch failed                  */
   LRD_ERR_UNSUPPORTED = -4, /* shape outside the compiled kernels' limits    */
-  LRD_ERR_NODEVICE = -5     /* no CUDA device / driver                       */
+  LRD_ERR_NODEVICE = -5,    /* no CUDA device / driver                       */
+  LRD_ERR_TIMEOUT = -6      /* a bounded device-side wait gave up            */
 };
+
+/* Bits of the device status word (lrd_workspace_status). */
+#define LRD_STATUS_TMA_TIMEOUT 1 /* a TMA completion wait exceeded its deadline */
 
 /* Arithmetic forms of the path. */
 enum lrd_form {
@@ -98,12 +102,19 @@ int lrd_denoise_host(const lrd_plan* plan, const float* h_vol, float* h_out, int
                      float* d_in, float* d_out, int32_t* d_ranks, void* d_workspace,
                      void* stream);
 
+/* Device status word of the last call that used ``d_workspace`` on
+ * ``stream``: 0, or LRD_STATUS_* bits set by kernels whose bounded waits gave
+ * up (the output of that call is then invalid). Synchronises ``stream``.
+ * lrd_denoise_host checks it itself and returns LRD_ERR_TIMEOUT. No
+ * counterpart in the reference (its kernels have no device-side waits). */
+int lrd_workspace_status(const lrd_plan* plan, const void* d_workspace, int32_t* status, void* stream);
+
 /* Stage entry points, for per-stage parity checks against step 4's unfused
  * route (step4_gram_eigh.py:60-67).
  *   lrd_stage_gram: G = Xc^T Xc for every patch -> d_gram (n_patches, nt, nt).
  *   lrd_stage_eigh: from d_gram, ascending eigenvalues -> d_lam (n_patches, nt)
- *     (nullable), the top-p eigenvectors in descending eigenvalue order as a
- *     compact row-major nt x p matrix at the start of each patch's nt*nt slot
+ *     (nullable), the top-p eigenvectors in descending eigenvalue order as the
+ *     rows of a compact p x nt block at the start of each patch's nt*nt slot
  *     of d_vecs, MP ranks -> d_ranks. d_gram is left unchanged. */
 int lrd_stage_gram(const lrd_plan* plan, const float* d_vol, float* d_gram, void* d_workspace,
                    void* stream);

@@ -19,6 +19,7 @@ LRD_ERR_NOMEM = -2
 LRD_ERR_CUDA = -3
 LRD_ERR_UNSUPPORTED = -4
 LRD_ERR_NODEVICE = -5
+LRD_ERR_TIMEOUT = -6
 
 FORMS = {"plain": 0, "accurate": 1}
 
@@ -40,6 +41,8 @@ SIGNATURES = {
     "lrd_plan_phase_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int32)]),
     "lrd_denoise_static": (ctypes.c_int, [ctypes.c_void_p] * 5),
+    "lrd_workspace_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.c_void_p]),
 }
 PHASES = ("center", "gram", "eigh_mp", "recon")
 
@@ -126,6 +129,12 @@ class Plan:
     def denoise_host(self, h_vol, h_out, h_ranks, d_in, d_out, d_ranks, d_ws, stream):
         check(load().lrd_denoise_host(self.handle, h_vol, h_out, h_ranks, d_in, d_out, d_ranks, d_ws,
                                       stream))
+
+    def status(self, d_ws: int, stream: int) -> int:
+        """Device status word of the last call on this workspace (syncs the stream)."""
+        st = ctypes.c_int32()
+        check(load().lrd_workspace_status(self.handle, d_ws, ctypes.byref(st), stream))
+        return int(st.value)
 
     def set_profiling(self, enable: bool):
         check(load().lrd_plan_set_profiling(self.handle, int(bool(enable))))

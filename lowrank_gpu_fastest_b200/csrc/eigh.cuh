@@ -7,7 +7,8 @@
 //  1. exact power-of-two scaling so the largest diagonal entry is in [0.5, 1);
 //  2. Householder reduction to tridiagonal form (lower, one reflector per
 //     column; the reflector vectors stay in the strictly-lower part);
-//  3. every eigenvalue by bisection on Sturm counts, one eigenvalue per lane;
+//  3. every eigenvalue by bisection on Sturm counts, two eigenvalues per lane
+//     evaluated as two interleaved dependency chains;
 //  4. the MP rank from the full spectrum, evaluated like step0_numpy_loop.py:
 //     18-24: eigs = float32(max(lambda, 0) / N) in descending order with the
 //     smallest (null) eigenvalue dropped (step4_gram_eigh.py:49), float32
@@ -15,16 +16,25 @@
 //       float64(float32(eigs_i - eigs_last)) * (t - i) * (N - i)
 //         > float64(float32(4 * rcum_i)) * sqrt(float64(t * N))
 //     counted over all i (NumPy promotes the ladder's test to float64);
-//  5. the top-p eigenvectors by inverse iteration on the tridiagonal matrix
-//     (partial-pivoting LU, three solves from distinct pseudo-random starts),
-//     modified Gram-Schmidt in descending eigenvalue order, then the
-//     Householder back-transform;
+//  5. the top-p eigenvectors, in chunks of 8: inverse iteration on the
+//     tridiagonal matrix (partial-pivoting LU, three solves from distinct
+//     pseudo-random starts), the Householder back-transform, then modified
+//     Gram-Schmidt in descending eigenvalue order;
 //  6. w = float32(1 / (2 + p)) (step0:36).
 //
-// Output per patch: the p eigenvectors as a compact row-major T x p matrix at
-// the start of the patch's T x T slot (the projector of step8:136 is V_p V_p^T; the reconstruction applies
-// it as (x V_p) V_p^T), the rank, the weight, optionally the ascending
-// eigenvalues.
+// The routine is templated on the working precision. The main pass runs it
+// in float32 on the float32 Gram. A patch whose MP test has an index with
+// |lhs/rhs - 1| below kRefineTol (a near-tie that float32 round-off could
+// decide either way) is queued, and eigh_refine_kernel redoes it in float64:
+// the Gram from exact float64 products of the float32 centred data with a
+// float64 sum, then the same eigen/MP/eigenvector steps in float64 - so
+// near-ties are decided as the float64 evaluation of the algorithm decides
+// them.
+//
+// Output per patch: the p eigenvectors (descending eigenvalue order) as the
+// rows of a compact p x T block at the start of the patch's T x T slot (the
+// projector of step8:136 is V_p V_p^T; the reconstruction applies it as
+// (x V_p) V_p^T), the rank, the weight, optionally the ascending eigenvalues.
 #pragma once
 
 #include <float.h>
@@ -33,34 +43,42 @@
 
 namespace lrd {
 
-__device__ __forceinline__ float warp_sum(float v) {
+template <typename Real>
+struct Num;
+template <>
+struct Num<float> {
+  static __device__ __forceinline__ float eps() { return FLT_EPSILON * 0.5f; }
+  static __device__ __forceinline__ float tiny() { return FLT_MIN; }
+  static __device__ __forceinline__ float huge() { return FLT_MAX; }
+  static __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+  static __device__ __forceinline__ float rsq(float a) { return rsqrtf(a); }
+};
+template <>
+struct Num<double> {
+  static __device__ __forceinline__ double eps() { return DBL_EPSILON * 0.5; }
+  static __device__ __forceinline__ double tiny() { return DBL_MIN; }
+  static __device__ __forceinline__ double huge() { return DBL_MAX; }
+  static __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+  static __device__ __forceinline__ double rsq(double a) { return rsqrt(a); }
+};
+
+template <typename Real>
+__device__ __forceinline__ Real warp_sum(Real v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-__device__ __forceinline__ float warp_max(float v) {
+template <typename Real>
+__device__ __forceinline__ Real warp_max(Real v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
-__device__ __forceinline__ float warp_min(float v) {
+template <typename Real>
+__device__ __forceinline__ Real warp_min(Real v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
-}
-
-// Number of eigenvalues of the tridiagonal (d, e^2) smaller than x.
-__device__ __forceinline__ int sturm_count(const float* __restrict__ d, const float* __restrict__ e2,
-                                           int n, float x, float pivmin) {
-  float q = d[0] - x;
-  if (fabsf(q) < pivmin) q = -pivmin;
-  int c = q < 0.f;
-  for (int i = 1; i < n; ++i) {
-    q = (d[i] - x) - __fdividef(e2[i - 1], q);
-    if (fabsf(q) < pivmin) q = -pivmin;
-    c += q < 0.f;
-  }
-  return c;
 }
 
 // Deterministic start vector entry in [-1, 1) for inverse iteration.
@@ -75,47 +93,66 @@ __device__ __forceinline__ float start_entry(int i, int j) {
 }
 
 constexpr int kInvGroup = 8;  // eigenvectors refined concurrently (one lane each)
+constexpr int kLdy = kInvGroup + 1;  // eigenvector chunk row stride
+constexpr double kRefineTol = 1e-4;  // MP-test margin below which float64 redoes the patch
 
 __host__ __device__ inline int eigh_lda(int n) { return n + ((n & 1) ? 2 : 1); }
 
-// Shared-memory floats per warp.
-__host__ __device__ inline size_t eigh_smem_floats(int n) {
-  const int lda = eigh_lda(n);
-  return (size_t)2 * n * lda + 5 * (size_t)n + (size_t)5 * n * kInvGroup;
+// Shared-memory elements (of the working type) per warp: A (n x lda),
+// eigenvector chunk (n x kLdy), d, e, e2, tau, lam (5n), LU of the chunk's
+// shifted tridiagonals (4 n kInvGroup).
+__host__ __device__ inline size_t eigh_smem_elems(int n) {
+  return (size_t)n * eigh_lda(n) + (size_t)n * kLdy + 5 * (size_t)n + (size_t)4 * n * kInvGroup;
+}
+__host__ __device__ inline size_t eigh_smem_floats(int n) { return eigh_smem_elems(n); }
+
+// Sturm counts of two shifts at once (two independent dependency chains per lane).
+template <typename Real>
+__device__ __forceinline__ void sturm_count2(const Real* __restrict__ d, const Real* __restrict__ e2, int n, Real x0,
+                                             Real x1, Real pivmin, int& c0, int& c1) {
+  Real q0 = d[0] - x0, q1 = d[0] - x1;
+  if (fabs(q0) < pivmin) q0 = -pivmin;
+  if (fabs(q1) < pivmin) q1 = -pivmin;
+  int a0 = q0 < Real(0), a1 = q1 < Real(0);
+  for (int i = 1; i < n; ++i) {
+    const Real di = d[i], ei = e2[i - 1];
+    q0 = (di - x0) - Num<Real>::fdiv(ei, q0);
+    q1 = (di - x1) - Num<Real>::fdiv(ei, q1);
+    if (fabs(q0) < pivmin) q0 = -pivmin;
+    if (fabs(q1) < pivmin) q1 = -pivmin;
+    a0 += q0 < Real(0);
+    a1 += q1 < Real(0);
+  }
+  c0 = a0;
+  c1 = a1;
 }
 
-// grid: one block of 32 threads per patch. ``gram`` (read) and ``vecs``
-// (written) may alias: the block reads its whole matrix before writing.
-__global__ void __launch_bounds__(32)
-    eigh_mp_kernel(const float* gram, float* vecs, float* __restrict__ lam_out,
-                   int32_t* __restrict__ ranks, float* __restrict__ wgt, int n, int nvox) {
-  extern __shared__ float sm_eig[];
-  const int lane = threadIdx.x;
-  const long long b = blockIdx.x;
+// One warp: eigen-decomposition of the symmetric n x n matrix the caller put
+// in the first n*lda elements of ``sm``, MP rank and weight, top-p
+// eigenvectors (rows of the compact p x n block ``V``), optionally the
+// ascending eigenvalues. Returns the smallest |lhs/rhs - 1| of the MP test.
+template <typename Real>
+__device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_out, int32_t* rank_out,
+                               float* w_out) {
+  const int lane = threadIdx.x & 31;
   const int lda = eigh_lda(n);
-  float* A = sm_eig;             // n x lda, symmetric working matrix
-  float* Y = A + n * lda;        // n x lda, eigenvector j in column j
-  float* d = Y + n * lda;        // tridiagonal diagonal
-  float* e = d + n;              // sub-diagonal e[0..n-2]
-  float* e2 = e + n;             // e^2
-  float* tau = e2 + n;           // reflector scalars
-  float* lam = tau + n;          // ascending eigenvalues (scaled)
-  float* W = lam + n;            // scratch: 5 * n * kInvGroup floats
+  Real* A = sm;                  // n x lda, symmetric working matrix
+  Real* Y = A + n * lda;         // n x kLdy, current chunk of eigenvectors
+  Real* d = Y + n * kLdy;        // tridiagonal diagonal
+  Real* e = d + n;               // sub-diagonal e[0..n-2]
+  Real* e2 = e + n;              // e^2
+  Real* tau = e2 + n;            // reflector scalars
+  Real* lam = tau + n;           // ascending eigenvalues (scaled)
+  Real* W = lam + n;             // scratch: 4 * n * kInvGroup elements
+  const Real eps = Num<Real>::eps();
 
-  // ---- load and scale -----------------------------------------------------
-  const float* G = gram + b * (long long)n * n;
-  float dmax = 0.f;
-  for (int idx = lane; idx < n * n; idx += 32) {
-    const int r = idx / n, c = idx - r * n;
-    const float v = G[idx];
-    A[r * lda + c] = v;
-    if (r == c) dmax = fmaxf(dmax, fabsf(v));
-  }
+  // ---- exact power-of-two scaling -------------------------------------------
+  Real dmax = 0;
+  for (int i = lane; i < n; i += 32) dmax = fmax(dmax, fabs(A[i * lda + i]));
   dmax = warp_max(dmax);
   int ex = 0;
-  if (dmax > 0.f && isfinite(dmax)) frexpf(dmax, &ex);
-  const float scale = ldexpf(1.f, -ex), unscale = ldexpf(1.f, ex);
-  __syncwarp();
+  if (dmax > Real(0) && isfinite(dmax)) frexp(dmax, &ex);
+  const Real scale = ldexp(Real(1), -ex), unscale = ldexp(Real(1), ex);
   for (int idx = lane; idx < n * n; idx += 32) {
     const int r = idx / n, c = idx - r * n;
     A[r * lda + c] *= scale;
@@ -123,23 +160,23 @@ __global__ void __launch_bounds__(32)
   __syncwarp();
 
   // ---- Householder tridiagonalisation ---------------------------------------
-  float* vv = W;
-  float* pp = W + n;
-  float* ww = W + 2 * n;
+  Real* vv = W;
+  Real* pp = W + n;
+  Real* ww = W + 2 * n;
   for (int k = 0; k < n - 2; ++k) {
     const int L = n - k - 1;
-    float part = 0.f;
+    Real part = 0;
     for (int i = 1 + lane; i < L; i += 32) {
-      const float v = A[(k + 1 + i) * lda + k];
-      part = fmaf(v, v, part);
+      const Real v = A[(k + 1 + i) * lda + k];
+      part = fma(v, v, part);
     }
-    const float xnorm2 = warp_sum(part);
-    const float alpha = A[(k + 1) * lda + k];
-    float taui = 0.f, beta = alpha;
-    if (xnorm2 > 0.f) {
-      beta = -copysignf(sqrtf(fmaf(alpha, alpha, xnorm2)), alpha);
+    const Real xnorm2 = warp_sum(part);
+    const Real alpha = A[(k + 1) * lda + k];
+    Real taui = 0, beta = alpha;
+    if (xnorm2 > Real(0)) {
+      beta = -copysign(sqrt(fma(alpha, alpha, xnorm2)), alpha);
       taui = (beta - alpha) / beta;
-      const float sc = 1.f / (alpha - beta);
+      const Real sc = Real(1) / (alpha - beta);
       for (int i = 1 + lane; i < L; i += 32) A[(k + 1 + i) * lda + k] *= sc;
     }
     if (lane == 0) {
@@ -148,25 +185,32 @@ __global__ void __launch_bounds__(32)
       tau[k] = taui;
     }
     __syncwarp();
-    if (taui != 0.f) {
-      for (int i = lane; i < L; i += 32) vv[i] = (i == 0) ? 1.f : A[(k + 1 + i) * lda + k];
+    if (taui != Real(0)) {
+      for (int i = lane; i < L; i += 32) vv[i] = (i == 0) ? Real(1) : A[(k + 1 + i) * lda + k];
       __syncwarp();
       for (int i = lane; i < L; i += 32) {
-        const float* row = A + (k + 1 + i) * lda + (k + 1);
-        float s = 0.f;
-        for (int j = 0; j < L; ++j) s = fmaf(row[j], vv[j], s);
-        pp[i] = taui * s;
+        const Real* row = A + (k + 1 + i) * lda + (k + 1);
+        Real s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int j = 0;
+        for (; j + 4 <= L; j += 4) {
+          s0 = fma(row[j], vv[j], s0);
+          s1 = fma(row[j + 1], vv[j + 1], s1);
+          s2 = fma(row[j + 2], vv[j + 2], s2);
+          s3 = fma(row[j + 3], vv[j + 3], s3);
+        }
+        for (; j < L; ++j) s0 = fma(row[j], vv[j], s0);
+        pp[i] = taui * ((s0 + s1) + (s2 + s3));
       }
       __syncwarp();
-      float part2 = 0.f;
-      for (int i = lane; i < L; i += 32) part2 = fmaf(pp[i], vv[i], part2);
-      const float kc = -0.5f * taui * warp_sum(part2);
-      for (int i = lane; i < L; i += 32) ww[i] = fmaf(kc, vv[i], pp[i]);
+      Real part2 = 0;
+      for (int i = lane; i < L; i += 32) part2 = fma(pp[i], vv[i], part2);
+      const Real kc = Real(-0.5) * taui * warp_sum(part2);
+      for (int i = lane; i < L; i += 32) ww[i] = fma(kc, vv[i], pp[i]);
       __syncwarp();
       for (int i = lane; i < L; i += 32) {
-        const float vi = vv[i], wi = ww[i];
-        float* row = A + (k + 1 + i) * lda + (k + 1);
-        for (int j = 0; j < L; ++j) row[j] = fmaf(-vi, ww[j], fmaf(-wi, vv[j], row[j]));
+        const Real vi = vv[i], wi = ww[i];
+        Real* row = A + (k + 1 + i) * lda + (k + 1);
+        for (int j = 0; j < L; ++j) row[j] = fma(-vi, ww[j], fma(-wi, vv[j], row[j]));
       }
       __syncwarp();
     }
@@ -175,53 +219,71 @@ __global__ void __launch_bounds__(32)
     if (n >= 2) {
       d[n - 2] = A[(n - 2) * lda + (n - 2)];
       e[n - 2] = A[(n - 1) * lda + (n - 2)];
-      tau[n - 2] = 0.f;
+      tau[n - 2] = 0;
     }
     d[n - 1] = A[(n - 1) * lda + (n - 1)];
-    e[n - 1] = 0.f;
-    tau[n - 1] = 0.f;
+    e[n - 1] = 0;
+    tau[n - 1] = 0;
   }
   __syncwarp();
-  for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : 0.f;
+  for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : Real(0);
 
-  // ---- eigenvalues: bisection on Sturm counts -------------------------------
-  float glo = FLT_MAX, ghi = -FLT_MAX;
+  // ---- eigenvalues: bisection on Sturm counts, two chains per lane ----------
+  Real glo = Num<Real>::huge(), ghi = -Num<Real>::huge();
   for (int i = lane; i < n; i += 32) {
-    const float r = (i > 0 ? fabsf(e[i - 1]) : 0.f) + (i < n - 1 ? fabsf(e[i]) : 0.f);
-    glo = fminf(glo, d[i] - r);
-    ghi = fmaxf(ghi, d[i] + r);
+    const Real r = (i > 0 ? fabs(e[i - 1]) : Real(0)) + (i < n - 1 ? fabs(e[i]) : Real(0));
+    glo = fmin(glo, d[i] - r);
+    ghi = fmax(ghi, d[i] + r);
   }
   glo = warp_min(glo);
   ghi = warp_max(ghi);
-  const float tnorm = fmaxf(fmaxf(fabsf(glo), fabsf(ghi)), FLT_MIN);
-  const float eps = FLT_EPSILON * 0.5f;
-  glo -= 4.f * eps * tnorm * n;
-  ghi += 4.f * eps * tnorm * n;
-  const float pivmin = FLT_MIN * 4.f;
-  const float abstol = 0.1f * eps * tnorm;
+  const Real tnorm = fmax(fmax(fabs(glo), fabs(ghi)), Num<Real>::tiny());
+  glo -= Real(4) * eps * tnorm * n;
+  ghi += Real(4) * eps * tnorm * n;
+  const Real pivmin = Num<Real>::tiny() * Real(4);
+  const Real abstol = Real(0.1) * eps * tnorm;
   __syncwarp();
-  for (int j = lane; j < n; j += 32) {
-    float lo = glo, hi = ghi;
-    for (int it = 0; it < 80; ++it) {
-      const float tol = fmaxf(abstol, 2.f * eps * fmaxf(fabsf(lo), fabsf(hi)));
-      if (hi - lo <= tol) break;
-      const float mid = 0.5f * (lo + hi);
-      if (mid <= lo || mid >= hi) break;
-      if (sturm_count(d, e2, n, mid, pivmin) > j)
-        hi = mid;
-      else
-        lo = mid;
+  for (int j0 = lane; j0 < n; j0 += 64) {
+    const int j1 = j0 + 32;
+    const bool has1 = j1 < n;
+    Real lo0 = glo, hi0 = ghi, lo1 = glo, hi1 = ghi;
+    bool run0 = true, run1 = has1;
+    for (int it = 0; it < 200 && (run0 || run1); ++it) {
+      if (run0) {
+        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo0), fabs(hi0)));
+        const Real mid = Real(0.5) * (lo0 + hi0);
+        run0 = hi0 - lo0 > tol && mid > lo0 && mid < hi0;
+      }
+      if (run1) {
+        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo1), fabs(hi1)));
+        const Real mid = Real(0.5) * (lo1 + hi1);
+        run1 = hi1 - lo1 > tol && mid > lo1 && mid < hi1;
+      }
+      if (!run0 && !run1) break;
+      const Real m0 = Real(0.5) * (lo0 + hi0), m1 = Real(0.5) * (lo1 + hi1);
+      int c0, c1;
+      sturm_count2(d, e2, n, m0, m1, pivmin, c0, c1);
+      if (run0) {
+        if (c0 > j0) hi0 = m0; else lo0 = m0;
+      }
+      if (run1) {
+        if (c1 > j1) hi1 = m1; else lo1 = m1;
+      }
     }
-    lam[j] = 0.5f * (lo + hi);
+    lam[j0] = Real(0.5) * (lo0 + hi0);
+    if (has1) lam[j1] = Real(0.5) * (lo1 + hi1);
   }
   __syncwarp();
 
   // ---- MP rank (step0_numpy_loop.py:18-24) ---------------------------------
+  // eigs = float32(max(lambda, 0) / N), as step 0's float32 s**2 / n.
   const int t = n - 1;
-  float* eg = W;      // descending eigs, t entries
-  float* rc = W + n;  // suffix sums
-  for (int i = lane; i < t; i += 32)
-    eg[i] = __fdiv_rn(fmaxf(lam[n - 1 - i] * unscale, 0.f), (float)nvox);
+  float* eg = reinterpret_cast<float*>(W);   // descending eigs, t entries
+  float* rc = eg + n;                        // float32 suffix sums
+  for (int i = lane; i < t; i += 32) {
+    const Real l = fmax(lam[n - 1 - i] * unscale, Real(0));
+    eg[i] = (sizeof(Real) == 4) ? __fdiv_rn((float)l, (float)nvox) : (float)(l / (Real)nvox);
+  }
   __syncwarp();
   if (lane == 0) {
     float acc = eg[t - 1];
@@ -233,6 +295,7 @@ __global__ void __launch_bounds__(32)
   }
   __syncwarp();
   int p = 0;
+  double margin = DBL_MAX;
   {
     const double sq = sqrt((double)((long long)t * (long long)nvox));
     const float elast = eg[t - 1];
@@ -243,147 +306,256 @@ __global__ void __launch_bounds__(32)
         const double lhs = (double)__fsub_rn(eg[i], elast) * (double)(t - i) * (double)(nvox - i);
         const double rhs = (double)__fmul_rn(4.f, rc[i]) * sq;
         sig = lhs > rhs;
+        if (rhs > 0.0) margin = fmin(margin, fabs(lhs - rhs) / rhs);
       }
       p += __popc(__ballot_sync(0xffffffffu, sig));
     }
+    margin = warp_min(margin);
   }
   if (lane == 0) {
-    ranks[b] = p;
-    wgt[b] = (float)(1.0 / (2.0 + (double)p));
+    *rank_out = p;
+    *w_out = (float)(1.0 / (2.0 + (double)p));
   }
   if (lam_out != nullptr)
-    for (int i = lane; i < n; i += 32) lam_out[b * n + i] = lam[i] * unscale;
-  if (p == 0) return;
+    for (int i = lane; i < n; i += 32) lam_out[i] = (float)(lam[i] * unscale);
+  if (p == 0) return margin;
   __syncwarp();
 
-  // ---- top-p eigenvectors: inverse iteration on the tridiagonal -------------
-  const float pivtol = eps * tnorm;
-  float* U0 = W;
-  float* U1 = U0 + n * kInvGroup;
-  float* U2 = U1 + n * kInvGroup;
-  float* ML = U2 + n * kInvGroup;
-  float* SW = ML + n * kInvGroup;
+  // ---- top-p eigenvectors, in chunks of kInvGroup ---------------------------
+  // Each chunk: inverse iteration on the tridiagonal (one lane per vector),
+  // Householder back-transform (one lane per vector), then modified
+  // Gram-Schmidt in descending eigenvalue order against the vectors already
+  // written (earlier chunks, read back from the output) and the chunk's
+  // earlier vectors; the chunk is then written to the output, eigenvector k
+  // as row k of a compact p x n block.
+  const Real pivtol = eps * tnorm;
+  Real* RU0 = W;                     // reciprocal pivots
+  Real* U1 = RU0 + n * kInvGroup;    // first super-diagonal of U
+  Real* ML = U1 + n * kInvGroup;     // multipliers
+  Real* SW = ML + n * kInvGroup;     // row swaps (U's second super-diagonal is e[i+1] there)
   for (int j0 = 0; j0 < p; j0 += kInvGroup) {
     const int g = min(kInvGroup, p - j0);
     if (lane < g) {
-      const int j = j0 + lane;        // descending index
-      const float sig = lam[n - 1 - j];
       const int q = lane;
-      // LU with partial pivoting of (T - sig I)
-      float c = d[0] - sig, s = (n > 1) ? e[0] : 0.f;
+      const int j = j0 + q;  // descending index
+      const Real sig = lam[n - 1 - j];
+      Real c = d[0] - sig, s = (n > 1) ? e[0] : Real(0);
       for (int i = 0; i < n - 1; ++i) {
-        const float ei = e[i];
-        const float an = d[i + 1] - sig;
-        const float en = (i + 1 < n - 1) ? e[i + 1] : 0.f;
-        if (fabsf(c) >= fabsf(ei)) {
-          const float m = (ei == 0.f) ? 0.f : ei / c;
-          U0[i * kInvGroup + q] = c;
+        const Real ei = e[i];
+        const Real an = d[i + 1] - sig;
+        const Real en = (i + 1 < n - 1) ? e[i + 1] : Real(0);
+        Real piv;
+        if (fabs(c) >= fabs(ei)) {
+          const Real m = (ei == Real(0)) ? Real(0) : ei / c;
+          piv = c;
           U1[i * kInvGroup + q] = s;
-          U2[i * kInvGroup + q] = 0.f;
           ML[i * kInvGroup + q] = m;
-          SW[i * kInvGroup + q] = 0.f;
-          c = fmaf(-m, s, an);
+          SW[i * kInvGroup + q] = 0;
+          c = fma(-m, s, an);
           s = en;
         } else {
-          const float m = c / ei;
-          U0[i * kInvGroup + q] = ei;
+          const Real m = c / ei;
+          piv = ei;
           U1[i * kInvGroup + q] = an;
-          U2[i * kInvGroup + q] = en;
           ML[i * kInvGroup + q] = m;
-          SW[i * kInvGroup + q] = 1.f;
-          c = fmaf(-m, an, s);
+          SW[i * kInvGroup + q] = 1;
+          c = fma(-m, an, s);
           s = -m * en;
         }
+        if (fabs(piv) < pivtol) piv = (piv < Real(0)) ? -pivtol : pivtol;
+        RU0[i * kInvGroup + q] = Real(1) / piv;
       }
-      U0[(n - 1) * kInvGroup + q] = c;
-      for (int i = 0; i < n; ++i) {
-        const float u = U0[i * kInvGroup + q];
-        if (fabsf(u) < pivtol) U0[i * kInvGroup + q] = (u < 0.f) ? -pivtol : pivtol;
-      }
-      // start vector
-      for (int i = 0; i < n; ++i) Y[i * lda + j] = start_entry(i, j);
+      if (fabs(c) < pivtol) c = (c < Real(0)) ? -pivtol : pivtol;
+      RU0[(n - 1) * kInvGroup + q] = Real(1) / c;
+      for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
       for (int iter = 0; iter < 3; ++iter) {
         for (int i = 0; i < n - 1; ++i) {
-          const float bi = Y[i * lda + j], bi1 = Y[(i + 1) * lda + j];
-          const float m = ML[i * kInvGroup + q];
-          if (SW[i * kInvGroup + q] != 0.f) {
-            Y[i * lda + j] = bi1;
-            Y[(i + 1) * lda + j] = fmaf(-m, bi1, bi);
+          const Real bi = Y[i * kLdy + q], bi1 = Y[(i + 1) * kLdy + q];
+          const Real m = ML[i * kInvGroup + q];
+          if (SW[i * kInvGroup + q] != Real(0)) {
+            Y[i * kLdy + q] = bi1;
+            Y[(i + 1) * kLdy + q] = fma(-m, bi1, bi);
           } else {
-            Y[(i + 1) * lda + j] = fmaf(-m, bi, bi1);
+            Y[(i + 1) * kLdy + q] = fma(-m, bi, bi1);
           }
         }
-        float x2 = Y[(n - 1) * lda + j] / U0[(n - 1) * kInvGroup + q];
-        Y[(n - 1) * lda + j] = x2;
-        float x1 = x2, amax = fabsf(x2);
+        Real x2 = Y[(n - 1) * kLdy + q] * RU0[(n - 1) * kInvGroup + q];
+        Y[(n - 1) * kLdy + q] = x2;
+        Real x1 = x2, amax = fabs(x2);
         if (n >= 2) {
-          x1 = (Y[(n - 2) * lda + j] - U1[(n - 2) * kInvGroup + q] * x2) / U0[(n - 2) * kInvGroup + q];
-          Y[(n - 2) * lda + j] = x1;
-          amax = fmaxf(amax, fabsf(x1));
+          x1 = (Y[(n - 2) * kLdy + q] - U1[(n - 2) * kInvGroup + q] * x2) * RU0[(n - 2) * kInvGroup + q];
+          Y[(n - 2) * kLdy + q] = x1;
+          amax = fmax(amax, fabs(x1));
         }
         for (int i = n - 3; i >= 0; --i) {
-          const float xi = (Y[i * lda + j] - U1[i * kInvGroup + q] * x1 - U2[i * kInvGroup + q] * x2) /
-                           U0[i * kInvGroup + q];
-          Y[i * lda + j] = xi;
-          amax = fmaxf(amax, fabsf(xi));
+          const Real u2 = (SW[i * kInvGroup + q] != Real(0)) ? e[i + 1] : Real(0);
+          const Real xi = (Y[i * kLdy + q] - U1[i * kInvGroup + q] * x1 - u2 * x2) * RU0[i * kInvGroup + q];
+          Y[i * kLdy + q] = xi;
+          amax = fmax(amax, fabs(xi));
           x2 = x1;
           x1 = xi;
         }
         // normalise with a max-abs prescale (the solve can grow by 1/pivtol per
         // tiny pivot); a non-finite solve restarts from a fresh start vector
-        if (!(amax > 0.f) || !isfinite(amax)) {
-          for (int i = 0; i < n; ++i) Y[i * lda + j] = start_entry(i, j + 977 * (iter + 1));
+        if (!(amax > Real(0)) || !isfinite(amax)) {
+          for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
           continue;
         }
-        const float sa = 1.f / amax;
-        float nrm = 0.f;
+        const Real sa = Real(1) / amax;
+        Real nrm = 0;
         for (int i = 0; i < n; ++i) {
-          const float v = Y[i * lda + j] * sa;
-          Y[i * lda + j] = v;
-          nrm = fmaf(v, v, nrm);
+          const Real v = Y[i * kLdy + q] * sa;
+          Y[i * kLdy + q] = v;
+          nrm = fma(v, v, nrm);
         }
-        const float inv = rsqrtf(nrm);
-        for (int i = 0; i < n; ++i) Y[i * lda + j] *= inv;
+        const Real inv = Num<Real>::rsq(nrm);
+        for (int i = 0; i < n; ++i) Y[i * kLdy + q] *= inv;
+      }
+      // back-transform: x = H(0) H(1) ... H(n-3) y
+      for (int k = n - 3; k >= 0; --k) {
+        const Real tk = tau[k];
+        if (tk == Real(0)) continue;
+        const int L = n - k - 1;
+        Real dot = Y[(k + 1) * kLdy + q];
+        for (int i = 1; i < L; ++i) dot = fma(A[(k + 1 + i) * lda + k], Y[(k + 1 + i) * kLdy + q], dot);
+        const Real f = tk * dot;
+        Y[(k + 1) * kLdy + q] -= f;
+        for (int i = 1; i < L; ++i)
+          Y[(k + 1 + i) * kLdy + q] = fma(-f, A[(k + 1 + i) * lda + k], Y[(k + 1 + i) * kLdy + q]);
       }
     }
     __syncwarp();
-  }
-
-  // ---- modified Gram-Schmidt, descending eigenvalue order --------------------
-  for (int j = 0; j < p; ++j) {
-    for (int i = 0; i < j; ++i) {
-      float part = 0.f;
-      for (int r = lane; r < n; r += 32) part = fmaf(Y[r * lda + i], Y[r * lda + j], part);
-      const float dot = warp_sum(part);
-      for (int r = lane; r < n; r += 32) Y[r * lda + j] = fmaf(-dot, Y[r * lda + i], Y[r * lda + j]);
+    // modified Gram-Schmidt, then write the chunk
+    for (int q = 0; q < g; ++q) {
+      const int j = j0 + q;
+      for (int i = 0; i < j; ++i) {
+        Real part = 0;
+        if (i < j0) {
+          for (int r = lane; r < n; r += 32) part = fma((Real)V[i * n + r], Y[r * kLdy + q], part);
+        } else {
+          for (int r = lane; r < n; r += 32) part = fma(Y[r * kLdy + (i - j0)], Y[r * kLdy + q], part);
+        }
+        const Real dot = warp_sum(part);
+        if (i < j0) {
+          for (int r = lane; r < n; r += 32) Y[r * kLdy + q] = fma(-dot, (Real)V[i * n + r], Y[r * kLdy + q]);
+        } else {
+          for (int r = lane; r < n; r += 32) Y[r * kLdy + q] = fma(-dot, Y[r * kLdy + (i - j0)], Y[r * kLdy + q]);
+        }
+        __syncwarp();
+      }
+      Real part = 0;
+      for (int r = lane; r < n; r += 32) part = fma(Y[r * kLdy + q], Y[r * kLdy + q], part);
+      const Real inv = Num<Real>::rsq(fmax(warp_sum(part), Num<Real>::tiny()));
+      for (int r = lane; r < n; r += 32) Y[r * kLdy + q] *= inv;
       __syncwarp();
     }
-    float part = 0.f;
-    for (int r = lane; r < n; r += 32) part = fmaf(Y[r * lda + j], Y[r * lda + j], part);
-    const float inv = rsqrtf(fmaxf(warp_sum(part), FLT_MIN));
-    for (int r = lane; r < n; r += 32) Y[r * lda + j] *= inv;
+    for (int idx = lane; idx < n * g; idx += 32) {
+      const int c = idx / n, r = idx - c * n;
+      V[(j0 + c) * n + r] = (float)Y[r * kLdy + c];
+    }
     __syncwarp();
   }
+  return margin;
+}
 
-  // ---- back-transform: x = H(0) H(1) ... H(n-3) y, one lane per vector ------
-  for (int j = lane; j < p; j += 32) {
-    for (int k = n - 3; k >= 0; --k) {
-      const float tk = tau[k];
-      if (tk == 0.f) continue;
-      const int L = n - k - 1;
-      float dot = Y[(k + 1) * lda + j];
-      for (int i = 1; i < L; ++i) dot = fmaf(A[(k + 1 + i) * lda + k], Y[(k + 1 + i) * lda + j], dot);
-      const float f = tk * dot;
-      Y[(k + 1) * lda + j] -= f;
-      for (int i = 1; i < L; ++i) Y[(k + 1 + i) * lda + j] = fmaf(-f, A[(k + 1 + i) * lda + k], Y[(k + 1 + i) * lda + j]);
-    }
+// Main pass: one warp per patch, float32. grid: one block of 32 threads per
+// patch of this launch (patch index patch0 + blockIdx.x). ``gram`` (read) and
+// ``vecs`` (written) may alias: the block reads its whole matrix before
+// writing. Near-tie patches are appended to ``refine_ids`` (``refine_count``
+// entries, order not fixed) for eigh_refine_kernel.
+__global__ void __launch_bounds__(32)
+    eigh_mp_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
+                   float* __restrict__ wgt, int n, int nvox, long long patch0, int* __restrict__ refine_count,
+                   int* __restrict__ refine_ids) {
+  extern __shared__ float sm_eig[];
+  const int lane = threadIdx.x;
+  const long long b = blockIdx.x;
+  const int lda = eigh_lda(n);
+  const float* G = gram + b * (long long)n * n;
+  for (int idx = lane; idx < n * n; idx += 32) {
+    const int r = idx / n, c = idx - r * n;
+    sm_eig[r * lda + c] = G[idx];
   }
   __syncwarp();
-  // compact row-major n x p block at the start of the patch's n x n slot
-  float* V = vecs + b * (long long)n * n;
-  for (int idx = lane; idx < n * p; idx += 32) {
-    const int r = idx / p, c = idx - r * p;
-    V[idx] = Y[r * lda + c];
+  const double margin = eigh_mp_warp<float>(sm_eig, n, nvox, vecs + b * (long long)n * n,
+                                            lam_out ? lam_out + b * n : nullptr, ranks + b, wgt + b);
+  if (lane == 0 && refine_count != nullptr && margin < kRefineTol) {
+    const int slot = atomicAdd(refine_count, 1);
+    refine_ids[slot] = (int)(patch0 + b);
+  }
+}
+
+// Shared memory bytes of eigh_refine_kernel: the float64 eigensolver's arrays
+// plus one staged z-run of the patch (pz*T floats).
+__host__ __device__ inline size_t eigh_refine_smem_bytes(int n, int pz) {
+  return sizeof(double) * eigh_smem_elems(n) + sizeof(float) * (size_t)pz * n;
+}
+
+// Float64 pass over the queued near-tie patches: persistent grid, one patch
+// per block at a time. The block forms G = Xc^T Xc in float64 (products of the
+// float32 centred values are exact in float64, the sum is float64), then warp
+// 0 runs the float64 eigensolver and overwrites the patch's rank, weight,
+// eigenvectors (and eigenvalues if requested).
+__global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, float* __restrict__ lam_out,
+                                   int32_t* __restrict__ ranks, float* __restrict__ wgt, Geom g, AxisTables tab,
+                                   const int* __restrict__ refine_count, const int* __restrict__ refine_ids) {
+  extern __shared__ double sm_ref[];
+  const int n = g.nt;
+  const int lda = eigh_lda(n);
+  double* A = sm_ref;
+  float* run = reinterpret_cast<float*>(sm_ref + eigh_smem_elems(n));
+  const int count = *refine_count;
+  const int tid = threadIdx.x;
+  const int nth = blockDim.x;
+  const int nent = n * (n + 1) / 2;
+  for (int w = blockIdx.x; w < count; w += gridDim.x) {
+    const long long pid = refine_ids[w];
+    int ci, cj, ck;
+    patch_axes(g, pid, ci, cj, ck);
+    const int cx = tab.corners[0][ci], cy = tab.corners[1][cj], cz = tab.corners[2][ck];
+    for (int base = 0; base < nent; base += 8 * nth) {
+      int ei[8], ej[8];
+      bool live[8];
+      double acc[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        int e = base + tid + u * nth, r = 0;
+        live[u] = e < nent;
+        if (live[u])
+          while (e >= n - r) {
+            e -= n - r;
+            ++r;
+          }
+        ei[u] = live[u] ? r : 0;
+        ej[u] = live[u] ? r + e : 0;
+        acc[u] = 0.0;
+      }
+      for (int a = 0; a < g.px; ++a)
+        for (int bb = 0; bb < g.py; ++bb) {
+          __syncthreads();
+          const float* src = xc + voxel_row(g, cx + a, cy + bb, cz) * n;
+          for (int e = tid; e < g.pz * n; e += nth) run[e] = src[e];
+          __syncthreads();
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (!live[u]) continue;
+            double s_ = acc[u];
+            for (int rr = 0; rr < g.pz; ++rr) s_ = fma((double)run[rr * n + ei[u]], (double)run[rr * n + ej[u]], s_);
+            acc[u] = s_;
+          }
+        }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (!live[u]) continue;
+        A[ei[u] * lda + ej[u]] = acc[u];
+        A[ej[u] * lda + ei[u]] = acc[u];
+      }
+    }
+    __syncthreads();
+    if (tid < 32)
+      eigh_mp_warp<double>(A, n, g.nvox_patch, vecs + pid * (long long)n * n,
+                           lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid);
+    __syncthreads();
   }
 }
 

@@ -1,4 +1,6 @@
 // C ABI of the MP-PCA denoiser: plans, workspace, launches (include/lrd.h).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -12,6 +14,7 @@
 #include "center.cuh"
 #include "eigh.cuh"
 #include "gram.cuh"
+#include "gram_z.cuh"
 #include "lrd_common.cuh"
 #include "recon.cuh"
 
@@ -59,10 +62,15 @@ struct lrd_plan {
   long long nvox;
   int tpt;                 // recon frames per thread
   int gram_threads;
+  bool use_gramz;          // column Gram kernel (TMA-staged z-planes) instead of per-patch
+  int gramz_ring;          // window accumulator slots
+  size_t smem_gramz;
   size_t smem_center, smem_gram, smem_eigh, smem_recon;
   int center_warps;
   // workspace offsets (bytes)
-  size_t off_mean, off_xc, off_gv, off_rank, off_wgt, ws_bytes;
+  size_t off_mean, off_xc, off_gv, off_rank, off_wgt, off_status, off_refine, ws_bytes;
+  size_t smem_refine;
+  int refine_blocks;
   // device tables (one allocation)
   void* d_tables;
   lrd::AxisTables tab;
@@ -78,7 +86,7 @@ constexpr int kProfRing = 256;
 
 namespace {
 
-constexpr int kTptChoices[] = {4, 6, 8, 12, 16, 24, 32};
+constexpr int kTptChoices[] = {4, 8, 12, 16, 24, 32};
 
 int pick_tpt(int T) {
   const int need = (T + lrd::kReconSplit - 1) / lrd::kReconSplit;
@@ -107,6 +115,21 @@ BrickAxis brick_axis_cost(int size, int patch, const std::vector<int32_t>& corne
   return r;
 }
 
+// Largest number of patches touching one brick (the recon kernel stages their
+// ranks and weights in shared memory).
+int max_touch(const std::vector<int32_t> brick[3]) {
+  int best = 0;
+  for (size_t a = 0; a < brick[0].size() / 2; ++a)
+    for (size_t b = 0; b < brick[1].size() / 2; ++b)
+      for (size_t c = 0; c < brick[2].size() / 2; ++c) {
+        const int n = std::max(0, brick[0][2 * a + 1] - brick[0][2 * a] + 1) *
+                      std::max(0, brick[1][2 * b + 1] - brick[1][2 * b] + 1) *
+                      std::max(0, brick[2][2 * c + 1] - brick[2][2 * c] + 1);
+        best = std::max(best, n);
+      }
+  return best;
+}
+
 template <int TPT>
 void* recon_fn(bool accurate) {
   return accurate ? (void*)lrd::recon_kernel<TPT, true> : (void*)lrd::recon_kernel<TPT, false>;
@@ -115,7 +138,6 @@ void* recon_fn(bool accurate) {
 void* recon_kernel_ptr(int tpt, bool accurate) {
   switch (tpt) {
     case 4: return recon_fn<4>(accurate);
-    case 6: return recon_fn<6>(accurate);
     case 8: return recon_fn<8>(accurate);
     case 12: return recon_fn<12>(accurate);
     case 16: return recon_fn<16>(accurate);
@@ -149,8 +171,57 @@ int run_center(const lrd_plan* P, const float* d_vol, char* ws, cudaStream_t st)
   return launch_check("center_kernel launch");
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }
+  return fn;
+}
+
+// 4D tensor map over the centred volume (t, z, y, x), box (T, 1, py, px): one
+// z-plane of one patch column per TMA load.
+int encode_plane_map(const lrd_plan* P, const float* xc, CUtensorMap* map) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(LRD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const lrd::Geom& g = P->g;
+  const cuuint64_t dims[4] = {(cuuint64_t)g.nt, (cuuint64_t)g.nz, (cuuint64_t)g.ny, (cuuint64_t)g.nx};
+  const cuuint64_t strides[3] = {(cuuint64_t)g.nt * 4, (cuuint64_t)g.nz * g.nt * 4,
+                                 (cuuint64_t)g.ny * g.nz * g.nt * 4};
+  const cuuint32_t box[4] = {(cuuint32_t)g.nt, 1, (cuuint32_t)g.py, (cuuint32_t)g.px};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(xc), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(LRD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return LRD_OK;
+}
+
 int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
+  if (P->use_gramz) {
+    CUtensorMap map;
+    int rc = encode_plane_map(P, xc, &map);
+    if (rc) return rc;
+    int* status = reinterpret_cast<int*>(ws + P->off_status);
+    const long long ncol = (long long)P->g.ncx * P->g.ncy;
+    const long long cols = P->prob.batch > 0 ? std::max<long long>(1, P->prob.batch / P->g.ncz) : ncol;
+    const long long TT = (long long)P->g.nt * P->g.nt;
+    for (long long c0 = 0; c0 < ncol; c0 += cols) {
+      const long long nc = std::min(cols, ncol - c0);
+      lrd::gram_z_kernel<<<(unsigned)nc, P->gram_threads, P->smem_gramz, st>>>(
+          map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, status);
+      rc = launch_check("gram_z_kernel launch");
+      if (rc) return rc;
+    }
+    return LRD_OK;
+  }
   const long long npatch = P->g.npatch;
   const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
   const long long TT = (long long)P->g.nt * P->g.nt;
@@ -164,21 +235,30 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
   return LRD_OK;
 }
 
-int run_eigh(const lrd_plan* P, const float* d_gram, float* d_vecs, float* d_lam, int32_t* d_rank,
+// Float32 eigensolver over all patches, then the float64 pass over the
+// near-tie patches it queued (the queue lives in the workspace; the centred
+// volume there is the one the Gram was formed from).
+int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, float* d_lam, int32_t* d_rank,
              float* d_wgt, cudaStream_t st) {
   const long long npatch = P->g.npatch;
   const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
   const int T = P->g.nt;
   const long long TT = (long long)T * T;
+  int* rcount = reinterpret_cast<int*>(ws + P->off_refine);
+  int* rids = rcount + 64;
+  LRD_CUDA(cudaMemsetAsync(rcount, 0, sizeof(int), st));
   for (long long p0 = 0; p0 < npatch; p0 += batch) {
     const long long nb = std::min(batch, npatch - p0);
     lrd::eigh_mp_kernel<<<(unsigned)nb, 32, P->smem_eigh, st>>>(
         d_gram + p0 * TT, d_vecs + p0 * TT, d_lam ? d_lam + p0 * T : nullptr, d_rank + p0, d_wgt + p0,
-        T, P->g.nvox_patch);
+        T, P->g.nvox_patch, p0, rcount, rids);
     int rc = launch_check("eigh_mp_kernel launch");
     if (rc) return rc;
   }
-  return LRD_OK;
+  const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
+  lrd::eigh_refine_kernel<<<P->refine_blocks, 128, P->smem_refine, st>>>(xc, d_vecs, d_lam, d_rank, d_wgt, P->g,
+                                                                        P->tab, rcount, rids);
+  return launch_check("eigh_refine_kernel launch");
 }
 
 int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st) {
@@ -359,9 +439,25 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   P->smem_center = sizeof(float) * (size_t)P->center_warps * (32 * (T + 1) + 32);
   P->smem_gram = sizeof(float) * (size_t)pr->py * pr->pz * (4 * nb4);
   P->smem_eigh = sizeof(float) * lrd::eigh_smem_floats(T);
-  P->smem_recon = sizeof(float) * (size_t)T * (T | 1);
+  P->smem_recon = lrd::recon_smem_bytes(T, max_touch(brick));
+  {
+    int ring = 1;
+    for (int z = 0; z < pr->nz; ++z) ring = std::max(ring, cover[2][2 * z + 1] - cover[2][2 * z] + 1);
+    P->gramz_ring = ring;
+    P->smem_gramz = lrd::gramz_smem_bytes(pr->px * pr->py, T, ring, P->gram_threads);
+    P->use_gramz = (T % 4 == 0) && P->smem_gramz <= 200 * 1024 && tensor_map_encoder() != nullptr &&
+                   pr->px <= 256 && pr->py <= 256;
+  }
   int rc = set_smem((const void*)lrd::center_kernel, P->smem_center);
   if (!rc) rc = set_smem((const void*)lrd::gram_kernel, P->smem_gram);
+  if (!rc && P->use_gramz) rc = set_smem((const void*)lrd::gram_z_kernel, P->smem_gramz);
+  P->smem_refine = lrd::eigh_refine_smem_bytes(T, pr->pz);
+  if (!rc) rc = set_smem((const void*)lrd::eigh_refine_kernel, P->smem_refine);
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    P->refine_blocks = std::max(1, std::min<int>(2 * sms, (int)std::min<long long>(g.npatch, 1 << 20)));
+  }
   if (!rc) rc = set_smem((const void*)lrd::eigh_mp_kernel, P->smem_eigh);
   if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, false), P->smem_recon);
   if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, true), P->smem_recon);
@@ -370,7 +466,8 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
     delete P;
     return rc;
   }
-  if (P->smem_gram > 227 * 1024 || P->smem_eigh > 227 * 1024) {
+  if (P->smem_gram > 227 * 1024 || P->smem_eigh > 227 * 1024 || P->smem_recon > 227 * 1024 ||
+      P->smem_refine > 227 * 1024) {
     cudaFree(P->d_tables);
     delete P;
     return fail(LRD_ERR_UNSUPPORTED, "patch plane or T too large for shared memory");
@@ -383,6 +480,8 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   P->off_gv = off; off += align256(sizeof(float) * (size_t)g.npatch * T * T);
   P->off_rank = off; off += align256(sizeof(int32_t) * (size_t)g.npatch);
   P->off_wgt = off; off += align256(sizeof(float) * (size_t)g.npatch);
+  P->off_status = off; off += align256(sizeof(int32_t));
+  P->off_refine = off; off += align256(sizeof(int32_t) * (64 + (size_t)g.npatch));
   P->ws_bytes = off;
   *out = P;
   return LRD_OK;
@@ -460,11 +559,12 @@ int lrd_denoise(const lrd_plan* P, const float* d_vol, float* d_out, int32_t* d_
     ++const_cast<lrd_plan*>(P)->prof_calls;
   }
   if (ev) LRD_CUDA(cudaEventRecord(ev[0], st));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
   if ((rc = run_center(P, d_vol, ws, st))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[1], st));
   if ((rc = run_gram(P, ws, gv, st))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[2], st));
-  if ((rc = run_eigh(P, gv, gv, nullptr, rank, wgt, st))) return rc;
+  if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[3], st));
   if ((rc = run_recon(P, ws, d_out, st))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[4], st));
@@ -486,6 +586,20 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   if (h_ranks)
     LRD_CUDA(cudaMemcpyAsync(h_ranks, d_ranks, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToHost, st));
   LRD_CUDA(cudaStreamSynchronize(st));
+  int32_t status = 0;
+  if ((rc = lrd_workspace_status(P, d_ws, &status, stream))) return rc;
+  if (status) return fail(LRD_ERR_TIMEOUT, "a device wait gave up (status 0x%x): the result is invalid", status);
+  return LRD_OK;
+}
+
+int lrd_workspace_status(const lrd_plan* P, const void* d_ws, int32_t* status, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!d_ws || !status) return fail(LRD_ERR_INVALID, "NULL argument");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  LRD_CUDA(cudaMemcpyAsync(status, static_cast<const char*>(d_ws) + P->off_status, sizeof(int32_t),
+                           cudaMemcpyDeviceToHost, st));
+  LRD_CUDA(cudaStreamSynchronize(st));
   return LRD_OK;
 }
 
@@ -495,6 +609,7 @@ int lrd_stage_gram(const lrd_plan* P, const float* d_vol, float* d_gram, void* d
   if (!d_vol || !d_gram || !d_ws) return fail(LRD_ERR_INVALID, "NULL device buffer");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   char* ws = static_cast<char*>(d_ws);
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
   if ((rc = run_center(P, d_vol, ws, st))) return rc;
   return run_gram(P, ws, d_gram, st);
 }
@@ -508,7 +623,7 @@ int lrd_stage_eigh(const lrd_plan* P, const float* d_gram, float* d_lam, float* 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   char* ws = static_cast<char*>(d_ws);
   float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
-  return run_eigh(P, d_gram, d_vecs, d_lam, d_ranks, wgt, st);
+  return run_eigh(P, ws, d_gram, d_vecs, d_lam, d_ranks, wgt, st);
 }
 
 }  // extern "C"

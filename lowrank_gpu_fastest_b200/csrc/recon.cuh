@@ -15,13 +15,17 @@
 // patches to each voxel in exactly that order.
 //
 // Layout: one CTA per brick of bx*by*bz voxels, 4 threads per voxel (thread
-// ``s`` of a voxel owns frames t = s, s+4, s+8, ...). The CTA walks every patch
-// touching the brick in x-major order; the patch's eigenvector block V_p
-// (T x p, compact) is staged in shared memory; each thread computes its
-// partial y = (x - m)_slice . V_p, the 4 partials of a voxel are combined with
-// two shuffles, then xd = y V_p^T + m for its frames; a voxel the patch does
-// not cover skips the accumulation. Coverage is separable: per axis the
-// covering corner indices of a voxel form one contiguous range.
+// ``s`` of a voxel owns the contiguous frames [s*TPT, s*TPT + TPT) ∩ [0, T)).
+// The ranks and weights of every patch touching the brick are loaded once;
+// the CTA then walks those patches in x-major order with the eigenvector
+// block V_p (p x T, k-major, rows padded to a multiple of 4 floats) of the
+// next patch streamed into the other half of a shared-memory double buffer by
+// cp.async while the current one is used. Each thread computes its partial
+// y_k = (x - m)_slice . v_k from float4 reads of v_k, the 4 partials of a voxel
+// are combined with two shuffles, then xd = y V_p^T + m for its frames; a
+// voxel the patch does not cover skips the accumulation. Coverage is
+// separable: per axis the covering corner indices of a voxel form one
+// contiguous range.
 //
 // Form ACCURATE keeps the temporal mean out of the running sums: it
 // accumulates w * (x - m) V_p V_p^T with a compensated (two-sum) float32
@@ -42,20 +46,42 @@ __device__ __forceinline__ void two_sum_acc(float& acc, float& comp, float x) {
   acc = s;
 }
 
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float* smem_dst, const float* gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+__host__ __device__ inline int recon_tp(int T) { return (T + 3) & ~3; }
+
+// Dynamic shared memory bytes: two V buffers of T rows x recon_tp(T) floats,
+// then ranks (int) and weights (float) of up to max_touch patches.
+__host__ __device__ inline size_t recon_smem_bytes(int T, int max_touch) {
+  return sizeof(float) * 2 * (size_t)T * recon_tp(T) + (sizeof(int) + sizeof(float)) * (size_t)max_touch;
+}
+
 // grid: nbx*nby*nbz blocks of bx*by*bz*4 threads (<= 1024).
-// dynamic smem: T * (T | 1) floats (V tile, row stride p|1).
 template <int TPT, bool ACCURATE>
 __global__ void recon_kernel(const float* __restrict__ xc, const float* __restrict__ mean,
                              const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
                              const float* __restrict__ wgt, float* __restrict__ out, Geom g,
                              AxisTables tab) {
-  extern __shared__ float sV[];
-  __shared__ int s_p;
-  __shared__ float s_w;
+  extern __shared__ __align__(16) float sm_recon[];
   const int T = g.nt;
+  const int TP = recon_tp(T);
+  float* vbuf0 = sm_recon;
+  float* vbuf1 = sm_recon + (size_t)T * TP;
+  int* s_rank = reinterpret_cast<int*>(sm_recon + 2 * (size_t)T * TP);
   const int tid = threadIdx.x;
+  const int nthreads = blockDim.x;
   const int slice = tid & (kReconSplit - 1);
   const int vl = tid / kReconSplit;
+  const int t0 = slice * TPT;
 
   int brick = blockIdx.x;
   const int bzi = brick % g.nbz;
@@ -82,12 +108,30 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
   const int ilo = tab.brick[0][2 * bxi], ihi = tab.brick[0][2 * bxi + 1];
   const int jlo = tab.brick[1][2 * byi], jhi = tab.brick[1][2 * byi + 1];
   const int klo = tab.brick[2][2 * bzi], khi = tab.brick[2][2 * bzi + 1];
+  const int ni = max(0, ihi - ilo + 1), nj = max(0, jhi - jlo + 1), nk = max(0, khi - klo + 1);
+  const int np = ni * nj * nk;
+  float* s_w = reinterpret_cast<float*>(s_rank + np);
+
+  // ranks and weights of the touching patches, x-major order
+  for (int e = tid; e < np; e += nthreads) {
+    const int kk = e % nk, r = e / nk;
+    const int jj = r % nj, ii = r / nj;
+    const long long pid = ((long long)(ilo + ii) * g.ncy + (jlo + jj)) * g.ncz + (klo + kk);
+    s_rank[e] = ranks[pid];
+    s_w[e] = wgt[pid];
+  }
+  // zero the row padding of both buffers (never written by the copies)
+  if (TP != T)
+    for (int e = tid; e < 2 * T * (TP - T); e += nthreads) {
+      const int r = e / (TP - T), c = T + e % (TP - T);
+      sm_recon[(size_t)r * TP + c] = 0.f;
+    }
 
   float xr[TPT], acc[TPT], comp[TPT];
   float m = 0.f;
 #pragma unroll
   for (int u = 0; u < TPT; ++u) {
-    const int t = u * kReconSplit + slice;
+    const int t = t0 + u;
     xr[u] = (valid && t < T) ? xc[row * T + t] : 0.f;
     acc[u] = 0.f;
     comp[u] = 0.f;
@@ -95,65 +139,84 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
   if (valid) m = mean[row];
   float wacc = 0.f;
   double wacc64 = 0.0;
+  __syncthreads();
 
-  for (int i = ilo; i <= ihi; ++i) {
-    for (int j = jlo; j <= jhi; ++j) {
-      for (int k = klo; k <= khi; ++k) {
-        const long long pid = ((long long)i * g.ncy + j) * g.ncz + k;
-        __syncthreads();
-        if (tid == 0) {
-          s_p = ranks[pid];
-          s_w = wgt[pid];
-        }
-        __syncthreads();
-        const int p = s_p;
-        const float w = s_w;
-        const int ldv = p | 1;
-        {
-          const float* src = vecs + pid * (long long)T * T;
-          const int nv = T * p;
-          for (int e = tid; e < nv; e += blockDim.x) {
-            const int r = e / p, c = e - r * p;
-            sV[r * ldv + c] = src[e];
-          }
-        }
-        __syncthreads();
-        const bool cov = valid && i >= cxlo && i <= cxhi && j >= cylo && j <= cyhi && k >= czlo &&
-                         k <= czhi;
-        float xdp[TPT];
-#pragma unroll
-        for (int u = 0; u < TPT; ++u) xdp[u] = 0.f;
-        for (int kk = 0; kk < p; ++kk) {
-          float part = 0.f;
-#pragma unroll
-          for (int u = 0; u < TPT; ++u) {
-            const int t = u * kReconSplit + slice;
-            if (t < T) part = fmaf(xr[u], sV[t * ldv + kk], part);
-          }
-          part += __shfl_xor_sync(0xffffffffu, part, 1);
-          part += __shfl_xor_sync(0xffffffffu, part, 2);
-#pragma unroll
-          for (int u = 0; u < TPT; ++u) {
-            const int t = u * kReconSplit + slice;
-            if (t < T) xdp[u] = fmaf(part, sV[t * ldv + kk], xdp[u]);
-          }
-        }
-        if (cov) {
-          if (ACCURATE) {
-#pragma unroll
-            for (int u = 0; u < TPT; ++u) two_sum_acc(acc[u], comp[u], __fmul_rn(w, xdp[u]));
-            wacc64 += (double)w;
-          } else {
-#pragma unroll
-            for (int u = 0; u < TPT; ++u) {
-              const float xd = __fadd_rn(xdp[u], m);
-              acc[u] = __fadd_rn(acc[u], __fmul_rn(w, xd));
-            }
-            wacc = __fadd_rn(wacc, w);
-          }
-        }
+  const bool vec16 = (T & 3) == 0;
+  auto issue = [&](int kp, float* buf) {
+    const int kk = kp % nk, r = kp / nk;
+    const int jj = r % nj, ii = r / nj;
+    const long long pid = ((long long)(ilo + ii) * g.ncy + (jlo + jj)) * g.ncz + (klo + kk);
+    const int p = s_rank[kp];
+    const float* src = vecs + pid * (long long)T * T;
+    if (vec16) {
+      const int n4 = (T * p) >> 2;  // rows of T floats, T % 4 == 0, TP == T
+      for (int e = tid; e < n4; e += nthreads) cp_async16(buf + 4 * e, src + 4 * e);
+    } else {
+      const int nv = T * p;
+      for (int e = tid; e < nv; e += nthreads) {
+        const int k = e / T, t = e - k * T;
+        cp_async4(buf + (size_t)k * TP + t, src + e);
       }
     }
+  };
+
+  if (np > 0) issue(0, vbuf0);
+  cp_async_commit();
+  int ci = 0, cj = 0, ck = 0;  // axis offsets of patch kp within the brick's ranges
+  for (int kp = 0; kp < np; ++kp) {
+    if (kp + 1 < np) issue(kp + 1, ((kp + 1) & 1) ? vbuf1 : vbuf0);
+    cp_async_commit();
+    cp_async_wait1();
+    __syncthreads();
+    const float* vb = (kp & 1) ? vbuf1 : vbuf0;
+    const int p = s_rank[kp];
+    const float w = s_w[kp];
+    const int i = ilo + ci, j = jlo + cj, k = klo + ck;
+    const bool cov = valid && i >= cxlo && i <= cxhi && j >= cylo && j <= cyhi && k >= czlo && k <= czhi;
+    float xdp[TPT];
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) xdp[u] = 0.f;
+    for (int kk = 0; kk < p; ++kk) {
+      float v[TPT];
+      const float4* vr = reinterpret_cast<const float4*>(vb + (size_t)kk * TP + t0);
+#pragma unroll
+      for (int u4 = 0; u4 < TPT / 4; ++u4) {
+        const float4 q = (t0 + 4 * u4 < TP) ? vr[u4] : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[4 * u4 + 0] = q.x;
+        v[4 * u4 + 1] = q.y;
+        v[4 * u4 + 2] = q.z;
+        v[4 * u4 + 3] = q.w;
+      }
+      float part = 0.f;
+#pragma unroll
+      for (int u = 0; u < TPT; ++u) part = fmaf(xr[u], v[u], part);
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+#pragma unroll
+      for (int u = 0; u < TPT; ++u) xdp[u] = fmaf(part, v[u], xdp[u]);
+    }
+    if (cov) {
+      if (ACCURATE) {
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) two_sum_acc(acc[u], comp[u], __fmul_rn(w, xdp[u]));
+        wacc64 += (double)w;
+      } else {
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) {
+          const float xd = __fadd_rn(xdp[u], m);
+          acc[u] = __fadd_rn(acc[u], __fmul_rn(w, xd));
+        }
+        wacc = __fadd_rn(wacc, w);
+      }
+    }
+    if (++ck == nk) {
+      ck = 0;
+      if (++cj == nj) {
+        cj = 0;
+        ++ci;
+      }
+    }
+    __syncthreads();
   }
   if (!valid) return;
   if (ACCURATE) {
@@ -163,14 +226,14 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
     const double mm = wacc64 > 0.0 ? (double)m : 0.0;
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int t = u * kReconSplit + slice;
+      const int t = t0 + u;
       if (t < T) out[row * T + t] = (float)(mm + ((double)acc[u] + (double)comp[u]) * inv);
     }
   } else {
     const float den = fmaxf(wacc, 1e-12f);
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-      const int t = u * kReconSplit + slice;
+      const int t = t0 + u;
       if (t < T) out[row * T + t] = __fdiv_rn(acc[u], den);
     }
   }

@@ -147,7 +147,7 @@ def test_stage_gram_and_eigh_vs_fp64_oracle(cuda_ok):
         assert np.abs(lam[idx] - lam_ref).max() <= 1e-5 * np.abs(lam_ref).max()
         p = int(ranks[idx])
         assert p == st["p"]
-        V = vecs[idx].reshape(-1)[: T * p].reshape(T, p).astype(np.float64)
+        V = vecs[idx].reshape(-1)[: T * p].reshape(p, T).T.astype(np.float64)
         np.testing.assert_allclose(V.T @ V, np.eye(p), atol=1e-5)
         assert np.abs(V @ V.T - st["P"]).max() <= 1e-4
 
