@@ -55,14 +55,18 @@ enum lrd_form {
 };
 
 /* One problem: volume (nx, ny, nz, nt), patch (px, py, pz), one stride for the
- * three spatial axes (common.py:28-29, 37-44), the form, and ``batch`` = patches
- * per Gram/eigensolver launch (step8_tuned.py:21; 0 = all in one launch). */
+ * three spatial axes (common.py:28-29, 37-44), the form, ``batch`` = patches
+ * per Gram/eigensolver launch (step8_tuned.py:21; 0 = all in one launch), and
+ * the reconstruction brick (voxels per CTA along x, y, z; 0 = chosen by the
+ * plan's cost model; the autotuner fills it in). The brick changes speed only:
+ * every voxel's arithmetic and accumulation order are the same for any brick. */
 typedef struct lrd_problem {
   int32_t nx, ny, nz, nt;
   int32_t px, py, pz;
   int32_t stride;
   int32_t form;
   int32_t batch;
+  int32_t brick_x, brick_y, brick_z;
 } lrd_problem;
 
 typedef struct lrd_plan lrd_plan;

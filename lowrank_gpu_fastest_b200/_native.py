@@ -51,7 +51,8 @@ class LrdProblem(ctypes.Structure):
     """``struct lrd_problem`` (include/lrd.h)."""
 
     _fields_ = [(n, ctypes.c_int32) for n in
-                ("nx", "ny", "nz", "nt", "px", "py", "pz", "stride", "form", "batch")]
+                ("nx", "ny", "nz", "nt", "px", "py", "pz", "stride", "form", "batch",
+                 "brick_x", "brick_y", "brick_z")]
 
 
 class LrdError(RuntimeError):
@@ -93,13 +94,15 @@ def check(rc: int):
 class Plan:
     """Owns an ``lrd_plan*`` for one problem on the current CUDA device."""
 
-    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0):
+    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None):
         lib = load()
         if form not in FORMS:
             raise ValueError(f"form must be one of {sorted(FORMS)}, got {form!r}")
         nx, ny, nz, nt = (int(s) for s in shape)
         px, py, pz = (int(p) for p in patch)
-        self.problem = LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0))
+        bx, by, bz = (int(b) for b in (brick or (0, 0, 0)))
+        self.problem = LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0),
+                                  bx, by, bz)
         self.shape = (nx, ny, nz, nt)
         self.patch = (px, py, pz)
         self.stride = int(stride)

@@ -30,13 +30,14 @@ _workspaces: dict = {}
 _lock = threading.Lock()
 
 
-def _plan(shape, patch, stride, form, batch, device):
-    key = (tuple(shape), tuple(patch), int(stride), form, int(batch or 0), device)
+def _plan(shape, patch, stride, form, batch, device, brick=None):
+    key = (tuple(shape), tuple(patch), int(stride), form, int(batch or 0), device,
+           tuple(brick) if brick else None)
     with _lock:
         p = _plans.get(key)
         if p is None:
             with torch.cuda.device(device):
-                p = _native.Plan(shape, patch, stride, form, batch or 0)
+                p = _native.Plan(shape, patch, stride, form, batch or 0, brick)
             _plans[key] = p
     return p
 
@@ -51,11 +52,11 @@ def _workspace(plan, device, stream):
     return ws
 
 
-def get_plan(shape, patch=(11, 11, 11), stride=3, form="plain", batch=None, device=None):
+def get_plan(shape, patch=(11, 11, 11), stride=3, form="plain", batch=None, device=None, brick=None):
     """The cached native plan for a problem (creates it on first use)."""
     if device is None:
         device = torch.cuda.current_device()
-    return _plan(shape, patch, stride, form, batch, device)
+    return _plan(shape, patch, stride, form, batch, device, brick)
 
 
 def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", return_ranks=False,

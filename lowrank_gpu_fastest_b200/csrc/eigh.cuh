@@ -127,6 +127,109 @@ __device__ __forceinline__ void sturm_count2(const Real* __restrict__ d, const R
   c1 = a1;
 }
 
+// All eigenvalues of the symmetric tridiagonal (d, e) (e2 = e^2) by bisection
+// on Sturm counts, ascending into lam; two chains per lane. Returns the
+// Gerschgorin norm bound in tnorm. One warp.
+template <typename Real>
+__device__ void bisect_all(const Real* d, const Real* e, const Real* e2, Real* lam, int n, Real& tnorm_out) {
+  const int lane = threadIdx.x & 31;
+  const Real eps = Num<Real>::eps();
+  Real glo = Num<Real>::huge(), ghi = -Num<Real>::huge();
+  for (int i = lane; i < n; i += 32) {
+    const Real r = (i > 0 ? fabs(e[i - 1]) : Real(0)) + (i < n - 1 ? fabs(e[i]) : Real(0));
+    glo = fmin(glo, d[i] - r);
+    ghi = fmax(ghi, d[i] + r);
+  }
+  glo = warp_min(glo);
+  ghi = warp_max(ghi);
+  const Real tnorm = fmax(fmax(fabs(glo), fabs(ghi)), Num<Real>::tiny());
+  glo -= Real(4) * eps * tnorm * n;
+  ghi += Real(4) * eps * tnorm * n;
+  const Real pivmin = Num<Real>::tiny() * Real(4);
+  const Real abstol = Real(0.1) * eps * tnorm;
+  __syncwarp();
+  for (int j0 = lane; j0 < n; j0 += 64) {
+    const int j1 = j0 + 32;
+    const bool has1 = j1 < n;
+    Real lo0 = glo, hi0 = ghi, lo1 = glo, hi1 = ghi;
+    bool run0 = true, run1 = has1;
+    for (int it = 0; it < 200 && (run0 || run1); ++it) {
+      if (run0) {
+        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo0), fabs(hi0)));
+        const Real mid = Real(0.5) * (lo0 + hi0);
+        run0 = hi0 - lo0 > tol && mid > lo0 && mid < hi0;
+      }
+      if (run1) {
+        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo1), fabs(hi1)));
+        const Real mid = Real(0.5) * (lo1 + hi1);
+        run1 = hi1 - lo1 > tol && mid > lo1 && mid < hi1;
+      }
+      if (!run0 && !run1) break;
+      const Real m0 = Real(0.5) * (lo0 + hi0), m1 = Real(0.5) * (lo1 + hi1);
+      int c0, c1;
+      sturm_count2(d, e2, n, m0, m1, pivmin, c0, c1);
+      if (run0) {
+        if (c0 > j0) hi0 = m0; else lo0 = m0;
+      }
+      if (run1) {
+        if (c1 > j1) hi1 = m1; else lo1 = m1;
+      }
+    }
+    lam[j0] = Real(0.5) * (lo0 + hi0);
+    if (has1) lam[j1] = Real(0.5) * (lo1 + hi1);
+  }
+  __syncwarp();
+
+  tnorm_out = tnorm;
+}
+
+// MP rank from the ascending eigenvalues lam * unscale, evaluated like
+// step0_numpy_loop.py:18-24 (float32 eigs and suffix sums, float64 test,
+// a count over all indices); W holds 2n floats of scratch. Returns the
+// smallest |lhs/rhs - 1| over the indices. One warp.
+template <typename Real>
+__device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float* W, int& p_out) {
+  const int lane = threadIdx.x & 31;
+  // eigs = float32(max(lambda, 0) / N), as step 0's float32 s**2 / n.
+  const int t = n - 1;
+  float* eg = W;                             // descending eigs, t entries
+  float* rc = eg + n;                        // float32 suffix sums
+  for (int i = lane; i < t; i += 32) {
+    const Real l = fmax(lam[n - 1 - i] * unscale, Real(0));
+    eg[i] = (sizeof(Real) == 4) ? __fdiv_rn((float)l, (float)nvox) : (float)(l / (Real)nvox);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    float acc = eg[t - 1];
+    rc[t - 1] = acc;
+    for (int i = t - 2; i >= 0; --i) {
+      acc = __fadd_rn(acc, eg[i]);
+      rc[i] = acc;
+    }
+  }
+  __syncwarp();
+  int p = 0;
+  double margin = DBL_MAX;
+  {
+    const double sq = sqrt((double)((long long)t * (long long)nvox));
+    const float elast = eg[t - 1];
+    for (int i0 = 0; i0 < t; i0 += 32) {
+      const int i = i0 + lane;
+      bool sig = false;
+      if (i < t) {
+        const double lhs = (double)__fsub_rn(eg[i], elast) * (double)(t - i) * (double)(nvox - i);
+        const double rhs = (double)__fmul_rn(4.f, rc[i]) * sq;
+        sig = lhs > rhs;
+        if (rhs > 0.0) margin = fmin(margin, fabs(lhs - rhs) / rhs);
+      }
+      p += __popc(__ballot_sync(0xffffffffu, sig));
+    }
+    margin = warp_min(margin);
+  }
+  p_out = p;
+  return margin;
+}
+
 // One warp: eigen-decomposition of the symmetric n x n matrix the caller put
 // in the first n*lda elements of ``sm``, MP rank and weight, top-p
 // eigenvectors (rows of the compact p x n block ``V``), optionally the
@@ -228,90 +331,10 @@ __device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_o
   __syncwarp();
   for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : Real(0);
 
-  // ---- eigenvalues: bisection on Sturm counts, two chains per lane ----------
-  Real glo = Num<Real>::huge(), ghi = -Num<Real>::huge();
-  for (int i = lane; i < n; i += 32) {
-    const Real r = (i > 0 ? fabs(e[i - 1]) : Real(0)) + (i < n - 1 ? fabs(e[i]) : Real(0));
-    glo = fmin(glo, d[i] - r);
-    ghi = fmax(ghi, d[i] + r);
-  }
-  glo = warp_min(glo);
-  ghi = warp_max(ghi);
-  const Real tnorm = fmax(fmax(fabs(glo), fabs(ghi)), Num<Real>::tiny());
-  glo -= Real(4) * eps * tnorm * n;
-  ghi += Real(4) * eps * tnorm * n;
-  const Real pivmin = Num<Real>::tiny() * Real(4);
-  const Real abstol = Real(0.1) * eps * tnorm;
-  __syncwarp();
-  for (int j0 = lane; j0 < n; j0 += 64) {
-    const int j1 = j0 + 32;
-    const bool has1 = j1 < n;
-    Real lo0 = glo, hi0 = ghi, lo1 = glo, hi1 = ghi;
-    bool run0 = true, run1 = has1;
-    for (int it = 0; it < 200 && (run0 || run1); ++it) {
-      if (run0) {
-        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo0), fabs(hi0)));
-        const Real mid = Real(0.5) * (lo0 + hi0);
-        run0 = hi0 - lo0 > tol && mid > lo0 && mid < hi0;
-      }
-      if (run1) {
-        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo1), fabs(hi1)));
-        const Real mid = Real(0.5) * (lo1 + hi1);
-        run1 = hi1 - lo1 > tol && mid > lo1 && mid < hi1;
-      }
-      if (!run0 && !run1) break;
-      const Real m0 = Real(0.5) * (lo0 + hi0), m1 = Real(0.5) * (lo1 + hi1);
-      int c0, c1;
-      sturm_count2(d, e2, n, m0, m1, pivmin, c0, c1);
-      if (run0) {
-        if (c0 > j0) hi0 = m0; else lo0 = m0;
-      }
-      if (run1) {
-        if (c1 > j1) hi1 = m1; else lo1 = m1;
-      }
-    }
-    lam[j0] = Real(0.5) * (lo0 + hi0);
-    if (has1) lam[j1] = Real(0.5) * (lo1 + hi1);
-  }
-  __syncwarp();
-
-  // ---- MP rank (step0_numpy_loop.py:18-24) ---------------------------------
-  // eigs = float32(max(lambda, 0) / N), as step 0's float32 s**2 / n.
-  const int t = n - 1;
-  float* eg = reinterpret_cast<float*>(W);   // descending eigs, t entries
-  float* rc = eg + n;                        // float32 suffix sums
-  for (int i = lane; i < t; i += 32) {
-    const Real l = fmax(lam[n - 1 - i] * unscale, Real(0));
-    eg[i] = (sizeof(Real) == 4) ? __fdiv_rn((float)l, (float)nvox) : (float)(l / (Real)nvox);
-  }
-  __syncwarp();
-  if (lane == 0) {
-    float acc = eg[t - 1];
-    rc[t - 1] = acc;
-    for (int i = t - 2; i >= 0; --i) {
-      acc = __fadd_rn(acc, eg[i]);
-      rc[i] = acc;
-    }
-  }
-  __syncwarp();
-  int p = 0;
-  double margin = DBL_MAX;
-  {
-    const double sq = sqrt((double)((long long)t * (long long)nvox));
-    const float elast = eg[t - 1];
-    for (int i0 = 0; i0 < t; i0 += 32) {
-      const int i = i0 + lane;
-      bool sig = false;
-      if (i < t) {
-        const double lhs = (double)__fsub_rn(eg[i], elast) * (double)(t - i) * (double)(nvox - i);
-        const double rhs = (double)__fmul_rn(4.f, rc[i]) * sq;
-        sig = lhs > rhs;
-        if (rhs > 0.0) margin = fmin(margin, fabs(lhs - rhs) / rhs);
-      }
-      p += __popc(__ballot_sync(0xffffffffu, sig));
-    }
-    margin = warp_min(margin);
-  }
+  Real tnorm;
+  bisect_all<Real>(d, e, e2, lam, n, tnorm);
+  int p;
+  const double margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p);
   if (lane == 0) {
     *rank_out = p;
     *w_out = (float)(1.0 / (2.0 + (double)p));

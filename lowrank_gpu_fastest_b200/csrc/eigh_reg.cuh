@@ -1,0 +1,380 @@
+// Register-resident float32 eigensolver for T <= TMAX (TMAX in {32, 48, 64}).
+//
+// Same algorithm as eigh_mp_warp<float> (eigh.cuh) - Householder
+// tridiagonalisation, bisection, MP rank, inverse iteration, back-transform,
+// Gram-Schmidt - with the data placed for a warp:
+//
+//  * lane l holds rows l and l + 32 of the working matrix in registers
+//    (a[NR][TMAX], every column index compile-time), so the reflector's
+//    matrix-vector product and the rank-2 update touch no shared memory for
+//    the matrix itself; at step k the owner of row k broadcasts it through
+//    shared memory, which (by symmetry) is column k;
+//  * the reflector vectors are kept in shared memory (HV, one row per step,
+//    zero above the sub-diagonal and 1 on it) and double as the broadcast
+//    buffer of the matrix-vector product;
+//  * inverse iteration keeps its vector in registers (loops over the
+//    tridiagonal unrolled to TMAX), the LU factors in shared memory;
+//  * the back-transform and the Gram-Schmidt pass work on row-distributed
+//    vectors with warp reductions, 8 vectors at a time.
+//
+// The arithmetic follows the shared-memory routine up to the order of the
+// float32 sums, so the results agree to float32 round-off, and the same
+// near-tie test queues patches for the float64 pass.
+#pragma once
+
+#include "eigh.cuh"
+
+namespace lrd {
+
+template <int TMAX>
+__host__ __device__ constexpr int eigh_reg_nr() {
+  return (TMAX + 31) / 32;
+}
+
+// Shared-memory floats per warp: HV (TMAX x TMAX), row-k broadcast, w vector,
+// d, e, e2, tau, lam (5 TMAX), LU / MP scratch (4 TMAX kInvGroup), vector
+// transpose buffer (TMAX x kLdy).
+template <int TMAX>
+__host__ __device__ constexpr size_t eigh_reg_smem_floats() {
+  return (size_t)TMAX * TMAX + 2 * TMAX + 5 * TMAX + (size_t)4 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
+}
+
+template <int TMAX>
+__global__ void __launch_bounds__(32)
+    eigh_reg_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
+                    float* __restrict__ wgt, int n, int nvox, long long patch0, int* __restrict__ refine_count,
+                    int* __restrict__ refine_ids) {
+  constexpr int NR = eigh_reg_nr<TMAX>();
+  extern __shared__ __align__(16) float sr[];
+  float* HV = sr;                  // TMAX x TMAX reflector vectors
+  float* xk = HV + TMAX * TMAX;    // row k broadcast
+  float* ws = xk + TMAX;           // w vector broadcast
+  float* d = ws + TMAX;
+  float* e = d + TMAX;
+  float* e2 = e + TMAX;
+  float* tau = e2 + TMAX;
+  float* lam = tau + TMAX;
+  float* W = lam + TMAX;                 // LU (4 TMAX kInvGroup) / MP scratch (2 TMAX)
+  float* Yt = W + 4 * TMAX * kInvGroup;  // TMAX x kLdy
+  const int lane = threadIdx.x;
+  const long long b = blockIdx.x;
+  const float* G = gram + b * (long long)n * n;
+
+  // ---- load own rows, exact power-of-two scaling -----------------------------
+  float a[NR][TMAX];
+  float dmax = 0.f;
+#pragma unroll
+  for (int ri = 0; ri < NR; ++ri) {
+    const int r = lane + 32 * ri;
+    const bool rv = r < n;
+#pragma unroll
+    for (int j = 0; j < TMAX; ++j) a[ri][j] = (rv && j < n) ? G[(long long)r * n + j] : 0.f;
+    if (rv) dmax = fmaxf(dmax, fabsf(G[(long long)r * n + r]));
+  }
+  dmax = warp_max(dmax);
+  int ex = 0;
+  if (dmax > 0.f && isfinite(dmax)) frexpf(dmax, &ex);
+  const float scale = ldexpf(1.f, -ex), unscale = ldexpf(1.f, ex);
+#pragma unroll
+  for (int ri = 0; ri < NR; ++ri)
+#pragma unroll
+    for (int j = 0; j < TMAX; ++j) a[ri][j] *= scale;
+
+  // ---- Householder tridiagonalisation ---------------------------------------
+  for (int k = 0; k < n; ++k) {
+    // owner of row k broadcasts it (= column k by symmetry)
+    if (lane == (k & 31)) {
+      if (NR == 1 || k < 32) {
+#pragma unroll
+        for (int j = 0; j < TMAX; ++j) xk[j] = a[0][j];
+      } else {
+#pragma unroll
+        for (int j = 0; j < TMAX; ++j) xk[j] = a[NR - 1][j];
+      }
+    }
+    __syncwarp();
+    if (k >= n - 2) {
+      if (lane == 0) {
+        d[k] = xk[k];
+        e[k] = (k == n - 2) ? xk[k + 1] : 0.f;
+        tau[k] = 0.f;
+      }
+      __syncwarp();
+      continue;
+    }
+    float xr[NR];
+    float part = 0.f;
+#pragma unroll
+    for (int ri = 0; ri < NR; ++ri) {
+      const int r = lane + 32 * ri;
+      xr[ri] = (r < n) ? xk[r] : 0.f;
+      if (r >= k + 2 && r < n) part = fmaf(xr[ri], xr[ri], part);
+    }
+    const float xnorm2 = warp_sum(part);
+    const float alpha = xk[k + 1];
+    float taui = 0.f, beta = alpha, sc = 0.f;
+    if (xnorm2 > 0.f) {
+      beta = -copysignf(sqrtf(fmaf(alpha, alpha, xnorm2)), alpha);
+      taui = (beta - alpha) / beta;
+      sc = 1.f / (alpha - beta);
+    }
+    if (lane == 0) {
+      d[k] = xk[k];
+      e[k] = beta;
+      tau[k] = taui;
+    }
+    float* hv = HV + k * TMAX;
+    float vr[NR];
+#pragma unroll
+    for (int ri = 0; ri < NR; ++ri) {
+      const int r = lane + 32 * ri;
+      vr[ri] = (r == k + 1) ? 1.f : ((r >= k + 2 && r < n) ? xr[ri] * sc : 0.f);
+      if (r < TMAX) hv[r] = vr[ri];
+    }
+    __syncwarp();
+    if (taui != 0.f) {
+      // p = taui * A22 v over own rows (columns j >= k+1; hv is 0 below)
+      const int j4lo = (k + 1) >> 2;
+      float pr[NR];
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
+        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+        for (int j4 = 0; j4 < TMAX / 4; ++j4) {
+          if (j4 >= j4lo) {
+            const float4 v4 = reinterpret_cast<const float4*>(hv)[j4];
+            s0 = fmaf(a[ri][4 * j4 + 0], v4.x, s0);
+            s1 = fmaf(a[ri][4 * j4 + 1], v4.y, s1);
+            s2 = fmaf(a[ri][4 * j4 + 2], v4.z, s2);
+            s3 = fmaf(a[ri][4 * j4 + 3], v4.w, s3);
+          }
+        }
+        const int r = lane + 32 * ri;
+        pr[ri] = (r >= k + 1 && r < n) ? taui * ((s0 + s1) + (s2 + s3)) : 0.f;
+      }
+      float part2 = 0.f;
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) part2 = fmaf(pr[ri], vr[ri], part2);
+      const float kc = -0.5f * taui * warp_sum(part2);
+      float wr[NR];
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
+        const int r = lane + 32 * ri;
+        wr[ri] = fmaf(kc, vr[ri], pr[ri]);
+        if (r < TMAX) ws[r] = wr[ri];
+      }
+      __syncwarp();
+      // A22 -= v w^T + w v^T on own rows, columns j >= k+1 (ws, hv zero below)
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
+#pragma unroll
+        for (int j4 = 0; j4 < TMAX / 4; ++j4) {
+          if (j4 >= j4lo) {
+            const float4 v4 = reinterpret_cast<const float4*>(hv)[j4];
+            const float4 w4 = reinterpret_cast<const float4*>(ws)[j4];
+            a[ri][4 * j4 + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * j4 + 0]));
+            a[ri][4 * j4 + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * j4 + 1]));
+            a[ri][4 * j4 + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * j4 + 2]));
+            a[ri][4 * j4 + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * j4 + 3]));
+          }
+        }
+      }
+    }
+    __syncwarp();  // xk, ws are rewritten by the next step
+  }
+  for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : 0.f;
+  __syncwarp();
+
+  // ---- eigenvalues, MP rank ---------------------------------------------------
+  float tnorm;
+  bisect_all<float>(d, e, e2, lam, n, tnorm);
+  int p;
+  const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p);
+  if (lane == 0) {
+    ranks[b] = p;
+    wgt[b] = (float)(1.0 / (2.0 + (double)p));
+    if (refine_count != nullptr && margin < kRefineTol) refine_ids[atomicAdd(refine_count, 1)] = (int)(patch0 + b);
+  }
+  if (lam_out != nullptr)
+    for (int i = lane; i < n; i += 32) lam_out[b * n + i] = lam[i] * unscale;
+  if (p == 0) return;
+  __syncwarp();
+
+  // ---- top-p eigenvectors, 8 at a time --------------------------------------
+  const float pivtol = Num<float>::eps() * tnorm;
+  float* RU0 = W;
+  float* U1 = RU0 + TMAX * kInvGroup;
+  float* ML = U1 + TMAX * kInvGroup;
+  float* SW = ML + TMAX * kInvGroup;
+  float* V = vecs + b * (long long)n * n;
+  for (int j0 = 0; j0 < p; j0 += kInvGroup) {
+    const int g = min(kInvGroup, p - j0);
+    if (lane < g) {
+      const int q = lane;
+      const int j = j0 + q;
+      const float sig = lam[n - 1 - j];
+      // LU with partial pivoting of (T - sig I)
+      float c = d[0] - sig, s = (n > 1) ? e[0] : 0.f;
+      for (int i = 0; i < n - 1; ++i) {
+        const float ei = e[i];
+        const float an = d[i + 1] - sig;
+        const float en = (i + 1 < n - 1) ? e[i + 1] : 0.f;
+        float piv;
+        if (fabsf(c) >= fabsf(ei)) {
+          const float m = (ei == 0.f) ? 0.f : __fdividef(ei, c);
+          piv = c;
+          U1[i * kInvGroup + q] = s;
+          ML[i * kInvGroup + q] = m;
+          SW[i * kInvGroup + q] = 0.f;
+          c = fmaf(-m, s, an);
+          s = en;
+        } else {
+          const float m = __fdividef(c, ei);
+          piv = ei;
+          U1[i * kInvGroup + q] = an;
+          ML[i * kInvGroup + q] = m;
+          SW[i * kInvGroup + q] = 1.f;
+          c = fmaf(-m, an, s);
+          s = -m * en;
+        }
+        if (fabsf(piv) < pivtol) piv = (piv < 0.f) ? -pivtol : pivtol;
+        RU0[i * kInvGroup + q] = __fdividef(1.f, piv);
+      }
+      if (fabsf(c) < pivtol) c = (c < 0.f) ? -pivtol : pivtol;
+      RU0[(n - 1) * kInvGroup + q] = __fdividef(1.f, c);
+      float y[TMAX];
+#pragma unroll
+      for (int i = 0; i < TMAX; ++i) y[i] = (i < n) ? start_entry(i, j) : 0.f;
+      for (int iter = 0; iter < 3; ++iter) {
+#pragma unroll
+        for (int i = 0; i < TMAX - 1; ++i) {
+          if (i < n - 1) {
+            const float m = ML[i * kInvGroup + q];
+            if (SW[i * kInvGroup + q] != 0.f) {
+              const float bi = y[i];
+              y[i] = y[i + 1];
+              y[i + 1] = fmaf(-m, y[i + 1], bi);
+            } else {
+              y[i + 1] = fmaf(-m, y[i], y[i + 1]);
+            }
+          }
+        }
+        float amax = 0.f;
+#pragma unroll
+        for (int i = TMAX - 1; i >= 0; --i) {
+          if (i < n) {
+            const float y1 = (i + 1 < n && i + 1 < TMAX) ? y[(i + 1) % TMAX] : 0.f;
+            const float y2 = (i + 2 < n && i + 2 < TMAX) ? y[(i + 2) % TMAX] : 0.f;
+            const float u2 = (i + 1 < n - 1 && SW[i * kInvGroup + q] != 0.f) ? e[i + 1] : 0.f;
+            const float u1 = (i < n - 1) ? U1[i * kInvGroup + q] : 0.f;
+            y[i] = (y[i] - u1 * y1 - u2 * y2) * RU0[i * kInvGroup + q];
+            amax = fmaxf(amax, fabsf(y[i]));
+          }
+        }
+        if (!(amax > 0.f) || !isfinite(amax)) {
+#pragma unroll
+          for (int i = 0; i < TMAX; ++i) y[i] = (i < n) ? start_entry(i, j + 977 * (iter + 1)) : 0.f;
+          continue;
+        }
+        const float sa = 1.f / amax;
+        float nrm = 0.f;
+#pragma unroll
+        for (int i = 0; i < TMAX; ++i) {
+          y[i] *= sa;
+          nrm = fmaf(y[i], y[i], nrm);
+        }
+        const float inv = rsqrtf(nrm);
+#pragma unroll
+        for (int i = 0; i < TMAX; ++i) y[i] *= inv;
+      }
+#pragma unroll
+      for (int i = 0; i < TMAX; ++i)
+        if (i < n) Yt[i * kLdy + q] = y[i];
+    }
+    __syncwarp();
+    // row-distributed chunk: yr[ri][q] = vector q, row lane + 32 ri
+    float yr[NR][kInvGroup];
+#pragma unroll
+    for (int ri = 0; ri < NR; ++ri) {
+      const int r = lane + 32 * ri;
+#pragma unroll
+      for (int q = 0; q < kInvGroup; ++q) yr[ri][q] = (r < n && q < g) ? Yt[r * kLdy + q] : 0.f;
+    }
+    // back-transform x = H(0) ... H(n-3) y
+    for (int k = n - 3; k >= 0; --k) {
+      const float tk = tau[k];
+      if (tk == 0.f) continue;
+      float hr[NR];
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
+        const int r = lane + 32 * ri;
+        hr[ri] = (r < n) ? HV[k * TMAX + r] : 0.f;
+      }
+      float dq[kInvGroup];
+#pragma unroll
+      for (int q = 0; q < kInvGroup; ++q) {
+        float s_ = 0.f;
+#pragma unroll
+        for (int ri = 0; ri < NR; ++ri) s_ = fmaf(hr[ri], yr[ri][q], s_);
+        dq[q] = s_;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < kInvGroup; ++q) dq[q] += __shfl_xor_sync(0xffffffffu, dq[q], o);
+#pragma unroll
+      for (int q = 0; q < kInvGroup; ++q) {
+        const float f = tk * dq[q];
+#pragma unroll
+        for (int ri = 0; ri < NR; ++ri) yr[ri][q] = fmaf(-f, hr[ri], yr[ri][q]);
+      }
+    }
+    // modified Gram-Schmidt in descending eigenvalue order
+#pragma unroll
+    for (int q = 0; q < kInvGroup; ++q) {
+      if (q < g) {
+        for (int i = 0; i < j0; ++i) {  // earlier chunks, from the output
+          float s_ = 0.f;
+          float vi[NR];
+#pragma unroll
+          for (int ri = 0; ri < NR; ++ri) {
+            const int r = lane + 32 * ri;
+            vi[ri] = (r < n) ? V[i * n + r] : 0.f;
+            s_ = fmaf(vi[ri], yr[ri][q], s_);
+          }
+          const float dot = warp_sum(s_);
+#pragma unroll
+          for (int ri = 0; ri < NR; ++ri) yr[ri][q] = fmaf(-dot, vi[ri], yr[ri][q]);
+        }
+#pragma unroll
+        for (int i = 0; i < kInvGroup; ++i) {
+          if (i < q) {
+            float s_ = 0.f;
+#pragma unroll
+            for (int ri = 0; ri < NR; ++ri) s_ = fmaf(yr[ri][i], yr[ri][q], s_);
+            const float dot = warp_sum(s_);
+#pragma unroll
+            for (int ri = 0; ri < NR; ++ri) yr[ri][q] = fmaf(-dot, yr[ri][i], yr[ri][q]);
+          }
+        }
+        float s_ = 0.f;
+#pragma unroll
+        for (int ri = 0; ri < NR; ++ri) s_ = fmaf(yr[ri][q], yr[ri][q], s_);
+        const float inv = rsqrtf(fmaxf(warp_sum(s_), FLT_MIN));
+#pragma unroll
+        for (int ri = 0; ri < NR; ++ri) yr[ri][q] *= inv;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kInvGroup; ++q)
+      if (q < g)
+#pragma unroll
+        for (int ri = 0; ri < NR; ++ri) {
+          const int r = lane + 32 * ri;
+          if (r < n) V[(j0 + q) * n + r] = yr[ri][q];
+        }
+    __syncwarp();
+  }
+}
+
+}  // namespace lrd

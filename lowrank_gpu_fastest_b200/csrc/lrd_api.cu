@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -13,6 +14,7 @@
 #include "../../include/lrd.h"
 #include "center.cuh"
 #include "eigh.cuh"
+#include "eigh_reg.cuh"
 #include "gram.cuh"
 #include "gram_z.cuh"
 #include "lrd_common.cuh"
@@ -128,6 +130,48 @@ int max_touch(const std::vector<int32_t> brick[3]) {
         best = std::max(best, n);
       }
   return best;
+}
+
+// Default reconstruction brick: 64..128 threads per CTA (small CTAs keep
+// several resident per SM), fewest (voxel, touching patch) thread slots -
+// counting the idle lanes of a partial last warp - plus a small per-(brick,
+// patch) staging cost.
+void choose_brick(const int dims[3], const int pat[3], const std::vector<int32_t> corners[3], int best[3]) {
+  double best_cost = 1e300;
+  for (int bx = 1; bx <= 16; ++bx)
+    for (int by = 1; by <= 16; ++by)
+      for (int bz = 1; bz <= 32; ++bz) {
+        const int threads = bx * by * bz * lrd::kReconSplit;
+        if (threads < 64 || threads > 128) continue;
+        if ((bx > dims[0] && bx > 1) || (by > dims[1] && by > 1) || (bz > dims[2] && bz > 1)) continue;
+        const BrickAxis ax = brick_axis_cost(dims[0], pat[0], corners[0], bx);
+        const BrickAxis ay = brick_axis_cost(dims[1], pat[1], corners[1], by);
+        const BrickAxis az = brick_axis_cost(dims[2], pat[2], corners[2], bz);
+        const double pad = (double)((threads + 31) / 32 * 32) / threads;
+        const double touch = (double)ax.slots / bx * ay.slots / by * az.slots / bz;
+        const double cost = (double)ax.slots * ay.slots * az.slots * pad + 4.0 * touch;
+        if (cost < best_cost) {
+          best_cost = cost;
+          best[0] = bx;
+          best[1] = by;
+          best[2] = bz;
+        }
+      }
+}
+
+// Float32 eigensolver kernel and its shared-memory floats for frame count T:
+// the register-resident kernel up to T = 64, the shared-memory one above.
+size_t eigh_smem_for(int T) {
+  if (T <= 32) return lrd::eigh_reg_smem_floats<32>();
+  if (T <= 48) return lrd::eigh_reg_smem_floats<48>();
+  if (T <= 64) return lrd::eigh_reg_smem_floats<64>();
+  return lrd::eigh_smem_floats(T);
+}
+const void* eigh_kernel_for(int T) {
+  if (T <= 32) return (const void*)lrd::eigh_reg_kernel<32>;
+  if (T <= 48) return (const void*)lrd::eigh_reg_kernel<48>;
+  if (T <= 64) return (const void*)lrd::eigh_reg_kernel<64>;
+  return (const void*)lrd::eigh_mp_kernel;
 }
 
 template <int TPT>
@@ -249,10 +293,22 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
   LRD_CUDA(cudaMemsetAsync(rcount, 0, sizeof(int), st));
   for (long long p0 = 0; p0 < npatch; p0 += batch) {
     const long long nb = std::min(batch, npatch - p0);
-    lrd::eigh_mp_kernel<<<(unsigned)nb, 32, P->smem_eigh, st>>>(
-        d_gram + p0 * TT, d_vecs + p0 * TT, d_lam ? d_lam + p0 * T : nullptr, d_rank + p0, d_wgt + p0,
-        T, P->g.nvox_patch, p0, rcount, rids);
-    int rc = launch_check("eigh_mp_kernel launch");
+    const float* gin = d_gram + p0 * TT;
+    float* vout = d_vecs + p0 * TT;
+    float* lout = d_lam ? d_lam + p0 * T : nullptr;
+    if (T <= 32)
+      lrd::eigh_reg_kernel<32><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
+                                                                        P->g.nvox_patch, p0, rcount, rids);
+    else if (T <= 48)
+      lrd::eigh_reg_kernel<48><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
+                                                                        P->g.nvox_patch, p0, rcount, rids);
+    else if (T <= 64)
+      lrd::eigh_reg_kernel<64><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
+                                                                        P->g.nvox_patch, p0, rcount, rids);
+    else
+      lrd::eigh_mp_kernel<<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
+                                                                   P->g.nvox_patch, p0, rcount, rids);
+    int rc = launch_check("eigh kernel launch");
     if (rc) return rc;
   }
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
@@ -346,30 +402,16 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   }
   // brick shape
   int best[3] = {1, 1, 1};
-  double best_cost = 1e300;
-  for (int bx = 1; bx <= 16; ++bx)
-    for (int by = 1; by <= 16; ++by)
-      for (int bz = 1; bz <= 32; ++bz) {
-        const int threads = bx * by * bz * lrd::kReconSplit;
-        if (threads < 64 || threads > 512) continue;
-        if (bx > dims[0] + 0 && bx > 1) continue;
-        if (by > dims[1] && by > 1) continue;
-        if (bz > dims[2] && bz > 1) continue;
-        const BrickAxis ax = brick_axis_cost(dims[0], pat[0], corners[0], bx);
-        const BrickAxis ay = brick_axis_cost(dims[1], pat[1], corners[1], by);
-        const BrickAxis az = brick_axis_cost(dims[2], pat[2], corners[2], bz);
-        const long long nbr = (long long)ax.nblocks * ay.nblocks * az.nblocks;
-        // slots plus a per-(brick, patch) fixed cost (barriers, V staging)
-        const double touch = (double)ax.slots / bx * ay.slots / by * az.slots / bz;  // sum over bricks of touching patches
-        const double cost = (double)ax.slots * ay.slots * az.slots + touch * 64.0 +
-                            (nbr < 296 ? 1e18 / (double)nbr : 0.0);
-        if (cost < best_cost) {
-          best_cost = cost;
-          best[0] = bx;
-          best[1] = by;
-          best[2] = bz;
-        }
-      }
+  choose_brick(dims, pat, corners, best);
+  if (pr->brick_x > 0 || pr->brick_y > 0 || pr->brick_z > 0) {
+    if (pr->brick_x < 1 || pr->brick_y < 1 || pr->brick_z < 1 ||
+        (long long)pr->brick_x * pr->brick_y * pr->brick_z * lrd::kReconSplit > 1024)
+      return fail(LRD_ERR_INVALID, "brick %dx%dx%d: each side >= 1 and at most 256 voxels", pr->brick_x,
+                  pr->brick_y, pr->brick_z);
+    best[0] = pr->brick_x;
+    best[1] = pr->brick_y;
+    best[2] = pr->brick_z;
+  }
   const int bsz[3] = {best[0], best[1], best[2]};
   for (int a = 0; a < 3; ++a) {
     const int nb = (dims[a] + bsz[a] - 1) / bsz[a];
@@ -438,7 +480,7 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   P->center_warps = 4;
   P->smem_center = sizeof(float) * (size_t)P->center_warps * (32 * (T + 1) + 32);
   P->smem_gram = sizeof(float) * (size_t)pr->py * pr->pz * (4 * nb4);
-  P->smem_eigh = sizeof(float) * lrd::eigh_smem_floats(T);
+  P->smem_eigh = sizeof(float) * eigh_smem_for(T);
   P->smem_recon = lrd::recon_smem_bytes(T, max_touch(brick));
   {
     int ring = 1;
@@ -458,7 +500,7 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     P->refine_blocks = std::max(1, std::min<int>(2 * sms, (int)std::min<long long>(g.npatch, 1 << 20)));
   }
-  if (!rc) rc = set_smem((const void*)lrd::eigh_mp_kernel, P->smem_eigh);
+  if (!rc) rc = set_smem(eigh_kernel_for(T), P->smem_eigh);
   if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, false), P->smem_recon);
   if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, true), P->smem_recon);
   if (rc) {
