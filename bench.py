@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="patches in the CPU sample (0 = auto)")
     ap.add_argument("--brick", default=None, help="recon brick bx,by,bz (default: the plan's choice)")
+    ap.add_argument("--split", type=int, default=0, help="recon threads per voxel (0 = the plan's choice)")
     return ap.parse_args()
 
 
@@ -287,7 +288,7 @@ def run_ours(args, wl):
     d_vol = torch.from_numpy(vol).to(dev)
     d_out = torch.empty_like(d_vol)
     brick = tuple(int(v) for v in args.brick.split(",")) if args.brick else None
-    plan = api.get_plan(shape, patch, stride, form=args.form, device=local, brick=brick)
+    plan = api.get_plan(shape, patch, stride, form=args.form, device=local, brick=brick, split=args.split)
     ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=dev)
     d_ranks = torch.empty(plan.n_patches, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)

@@ -57,9 +57,10 @@ enum lrd_form {
 /* One problem: volume (nx, ny, nz, nt), patch (px, py, pz), one stride for the
  * three spatial axes (common.py:28-29, 37-44), the form, ``batch`` = patches
  * per Gram/eigensolver launch (step8_tuned.py:21; 0 = all in one launch), and
- * the reconstruction brick (voxels per CTA along x, y, z; 0 = chosen by the
- * plan's cost model; the autotuner fills it in). The brick changes speed only:
- * every voxel's arithmetic and accumulation order are the same for any brick. */
+ * the reconstruction brick (voxels per CTA along x, y, z) and threads per
+ * voxel (recon_split: 1, 2 or 4); 0 = chosen by the plan's cost model (the
+ * autotuner fills them in). These change speed only: every voxel's arithmetic
+ * and accumulation order are the same for any brick and split. */
 typedef struct lrd_problem {
   int32_t nx, ny, nz, nt;
   int32_t px, py, pz;
@@ -67,6 +68,7 @@ typedef struct lrd_problem {
   int32_t form;
   int32_t batch;
   int32_t brick_x, brick_y, brick_z;
+  int32_t recon_split;
 } lrd_problem;
 
 typedef struct lrd_plan lrd_plan;

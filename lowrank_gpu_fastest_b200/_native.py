@@ -52,7 +52,7 @@ class LrdProblem(ctypes.Structure):
 
     _fields_ = [(n, ctypes.c_int32) for n in
                 ("nx", "ny", "nz", "nt", "px", "py", "pz", "stride", "form", "batch",
-                 "brick_x", "brick_y", "brick_z")]
+                 "brick_x", "brick_y", "brick_z", "recon_split")]
 
 
 class LrdError(RuntimeError):
@@ -94,7 +94,7 @@ def check(rc: int):
 class Plan:
     """Owns an ``lrd_plan*`` for one problem on the current CUDA device."""
 
-    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None):
+    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0):
         lib = load()
         if form not in FORMS:
             raise ValueError(f"form must be one of {sorted(FORMS)}, got {form!r}")
@@ -102,7 +102,7 @@ class Plan:
         px, py, pz = (int(p) for p in patch)
         bx, by, bz = (int(b) for b in (brick or (0, 0, 0)))
         self.problem = LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0),
-                                  bx, by, bz)
+                                  bx, by, bz, int(split or 0))
         self.shape = (nx, ny, nz, nt)
         self.patch = (px, py, pz)
         self.stride = int(stride)

@@ -30,14 +30,14 @@ _workspaces: dict = {}
 _lock = threading.Lock()
 
 
-def _plan(shape, patch, stride, form, batch, device, brick=None):
+def _plan(shape, patch, stride, form, batch, device, brick=None, split=0):
     key = (tuple(shape), tuple(patch), int(stride), form, int(batch or 0), device,
-           tuple(brick) if brick else None)
+           tuple(brick) if brick else None, int(split or 0))
     with _lock:
         p = _plans.get(key)
         if p is None:
             with torch.cuda.device(device):
-                p = _native.Plan(shape, patch, stride, form, batch or 0, brick)
+                p = _native.Plan(shape, patch, stride, form, batch or 0, brick, split)
             _plans[key] = p
     return p
 
@@ -52,11 +52,12 @@ def _workspace(plan, device, stream):
     return ws
 
 
-def get_plan(shape, patch=(11, 11, 11), stride=3, form="plain", batch=None, device=None, brick=None):
+def get_plan(shape, patch=(11, 11, 11), stride=3, form="plain", batch=None, device=None, brick=None,
+             split=0):
     """The cached native plan for a problem (creates it on first use)."""
     if device is None:
         device = torch.cuda.current_device()
-    return _plan(shape, patch, stride, form, batch, device, brick)
+    return _plan(shape, patch, stride, form, batch, device, brick, split)
 
 
 def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", return_ranks=False,

@@ -26,6 +26,15 @@
 
 namespace lrd {
 
+#ifdef LRD_PHASE_CLOCKS
+__device__ long long* g_phase_clocks;  // 8 stamps per block, set by a probe build
+#define LRD_STAMP(i) \
+  do { __syncwarp(); if ((threadIdx.x & 31) == 0) g_phase_clocks[(long long)blockIdx.x * 8 + (i)] = clock64(); } while (0)
+#else
+#define LRD_STAMP(i) \
+  do { } while (0)
+#endif
+
 template <int TMAX>
 __host__ __device__ constexpr int eigh_reg_nr() {
   return (TMAX + 31) / 32;
@@ -59,6 +68,7 @@ __global__ void __launch_bounds__(32)
   const int lane = threadIdx.x;
   const long long b = blockIdx.x;
   const float* G = gram + b * (long long)n * n;
+  LRD_STAMP(0);
 
   // ---- load own rows, exact power-of-two scaling -----------------------------
   float a[NR][TMAX];
@@ -80,6 +90,7 @@ __global__ void __launch_bounds__(32)
 #pragma unroll
     for (int j = 0; j < TMAX; ++j) a[ri][j] *= scale;
 
+  LRD_STAMP(1);
   // ---- Householder tridiagonalisation ---------------------------------------
   for (int k = 0; k < n; ++k) {
     // owner of row k broadcasts it (= column k by symmetry)
@@ -185,9 +196,11 @@ __global__ void __launch_bounds__(32)
   for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : 0.f;
   __syncwarp();
 
+  LRD_STAMP(2);
   // ---- eigenvalues, MP rank ---------------------------------------------------
   float tnorm;
   bisect_all<float>(d, e, e2, lam, n, tnorm);
+  LRD_STAMP(3);
   int p;
   const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p);
   if (lane == 0) {
@@ -197,6 +210,7 @@ __global__ void __launch_bounds__(32)
   }
   if (lam_out != nullptr)
     for (int i = lane; i < n; i += 32) lam_out[b * n + i] = lam[i] * unscale;
+  LRD_STAMP(4);
   if (p == 0) return;
   __syncwarp();
 
@@ -292,6 +306,7 @@ __global__ void __launch_bounds__(32)
         if (i < n) Yt[i * kLdy + q] = y[i];
     }
     __syncwarp();
+    LRD_STAMP(5);
     // row-distributed chunk: yr[ri][q] = vector q, row lane + 32 ri
     float yr[NR][kInvGroup];
 #pragma unroll
@@ -329,6 +344,7 @@ __global__ void __launch_bounds__(32)
         for (int ri = 0; ri < NR; ++ri) yr[ri][q] = fmaf(-f, hr[ri], yr[ri][q]);
       }
     }
+    LRD_STAMP(6);
     // modified Gram-Schmidt in descending eigenvalue order
 #pragma unroll
     for (int q = 0; q < kInvGroup; ++q) {
@@ -375,6 +391,7 @@ __global__ void __launch_bounds__(32)
         }
     __syncwarp();
   }
+  LRD_STAMP(7);
 }
 
 }  // namespace lrd

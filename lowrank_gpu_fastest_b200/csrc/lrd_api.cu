@@ -63,6 +63,7 @@ struct lrd_plan {
   int device;
   long long nvox;
   int tpt;                 // recon frames per thread
+  int split;               // recon threads per voxel
   int gram_threads;
   bool use_gramz;          // column Gram kernel (TMA-staged z-planes) instead of per-patch
   int gramz_ring;          // window accumulator slots
@@ -88,13 +89,16 @@ constexpr int kProfRing = 256;
 
 namespace {
 
-constexpr int kTptChoices[] = {4, 8, 12, 16, 24, 32};
-
-int pick_tpt(int T) {
-  const int need = (T + lrd::kReconSplit - 1) / lrd::kReconSplit;
-  for (int c : kTptChoices)
-    if (c >= need) return c;
-  return -1;
+// Reconstruction thread layout for T frames: two threads per voxel up to
+// T = 96 (one shuffle per eigenvector; one thread per voxel needs ~220
+// registers at T = 48 and measured 3.4x slower), four above; frames per
+// thread rounded up to a multiple of 4 (float4 reads of the eigenvectors).
+void pick_recon_layout(int T, int want_split, int& split, int& tpt) {
+  split = T <= 96 ? 2 : 4;
+  if (want_split == 1 || want_split == 2 || want_split == 4) split = std::max(want_split, split);
+  tpt = ((T + split - 1) / split + 3) & ~3;
+  if (split == 2) tpt = std::max(tpt, 12);
+  if (split == 4) tpt = std::max(tpt, 8);
 }
 
 // Brick choice for the reconstruction: minimise the thread-slots the CTAs spend
@@ -132,17 +136,18 @@ int max_touch(const std::vector<int32_t> brick[3]) {
   return best;
 }
 
-// Default reconstruction brick: 64..128 threads per CTA (small CTAs keep
+// Default reconstruction brick: 27..128 threads per CTA (small CTAs keep
 // several resident per SM), fewest (voxel, touching patch) thread slots -
 // counting the idle lanes of a partial last warp - plus a small per-(brick,
 // patch) staging cost.
-void choose_brick(const int dims[3], const int pat[3], const std::vector<int32_t> corners[3], int best[3]) {
+void choose_brick(const int dims[3], const int pat[3], const std::vector<int32_t> corners[3], int split,
+                  int best[3]) {
   double best_cost = 1e300;
   for (int bx = 1; bx <= 16; ++bx)
     for (int by = 1; by <= 16; ++by)
       for (int bz = 1; bz <= 32; ++bz) {
-        const int threads = bx * by * bz * lrd::kReconSplit;
-        if (threads < 64 || threads > 128) continue;
+        const int threads = bx * by * bz * split;
+        if (threads < 27 || threads > 128) continue;
         if ((bx > dims[0] && bx > 1) || (by > dims[1] && by > 1) || (bz > dims[2] && bz > 1)) continue;
         const BrickAxis ax = brick_axis_cost(dims[0], pat[0], corners[0], bx);
         const BrickAxis ay = brick_axis_cost(dims[1], pat[1], corners[1], by);
@@ -174,19 +179,50 @@ const void* eigh_kernel_for(int T) {
   return (const void*)lrd::eigh_mp_kernel;
 }
 
-template <int TPT>
+template <int TPT, int SPLIT>
 void* recon_fn(bool accurate) {
-  return accurate ? (void*)lrd::recon_kernel<TPT, true> : (void*)lrd::recon_kernel<TPT, false>;
+  return accurate ? (void*)lrd::recon_kernel<TPT, SPLIT, true> : (void*)lrd::recon_kernel<TPT, SPLIT, false>;
 }
 
-void* recon_kernel_ptr(int tpt, bool accurate) {
-  switch (tpt) {
-    case 4: return recon_fn<4>(accurate);
-    case 8: return recon_fn<8>(accurate);
-    case 12: return recon_fn<12>(accurate);
-    case 16: return recon_fn<16>(accurate);
-    case 24: return recon_fn<24>(accurate);
-    case 32: return recon_fn<32>(accurate);
+void* recon_kernel_ptr(int tpt, int split, bool accurate) {
+  if (split == 1) {
+    switch (tpt) {
+      case 4: return recon_fn<4, 1>(accurate);
+      case 8: return recon_fn<8, 1>(accurate);
+      case 12: return recon_fn<12, 1>(accurate);
+      case 16: return recon_fn<16, 1>(accurate);
+      case 20: return recon_fn<20, 1>(accurate);
+      case 24: return recon_fn<24, 1>(accurate);
+      case 28: return recon_fn<28, 1>(accurate);
+      case 32: return recon_fn<32, 1>(accurate);
+      case 36: return recon_fn<36, 1>(accurate);
+      case 40: return recon_fn<40, 1>(accurate);
+      case 44: return recon_fn<44, 1>(accurate);
+      case 48: return recon_fn<48, 1>(accurate);
+    }
+  } else if (split == 2) {
+    switch (tpt) {
+      case 12: return recon_fn<12, 2>(accurate);
+      case 16: return recon_fn<16, 2>(accurate);
+      case 20: return recon_fn<20, 2>(accurate);
+      case 24: return recon_fn<24, 2>(accurate);
+      case 28: return recon_fn<28, 2>(accurate);
+      case 32: return recon_fn<32, 2>(accurate);
+      case 36: return recon_fn<36, 2>(accurate);
+      case 40: return recon_fn<40, 2>(accurate);
+      case 44: return recon_fn<44, 2>(accurate);
+      case 48: return recon_fn<48, 2>(accurate);
+    }
+  } else if (split == 4) {
+    switch (tpt) {
+      case 8: return recon_fn<8, 4>(accurate);
+      case 12: return recon_fn<12, 4>(accurate);
+      case 16: return recon_fn<16, 4>(accurate);
+      case 20: return recon_fn<20, 4>(accurate);
+      case 24: return recon_fn<24, 4>(accurate);
+      case 28: return recon_fn<28, 4>(accurate);
+      case 32: return recon_fn<32, 4>(accurate);
+    }
   }
   return nullptr;
 }
@@ -325,8 +361,8 @@ int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st) {
   const float* wgt = reinterpret_cast<const float*>(ws + P->off_wgt);
   const bool acc = P->prob.form == LRD_FORM_ACCURATE;
   const unsigned nbricks = (unsigned)((long long)P->g.nbx * P->g.nby * P->g.nbz);
-  const unsigned threads = (unsigned)(P->g.bx * P->g.by * P->g.bz * lrd::kReconSplit);
-  void* fn = recon_kernel_ptr(P->tpt, acc);
+  const unsigned threads = (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
+  void* fn = recon_kernel_ptr(P->tpt, P->split, acc);
   lrd::Geom g = P->g;
   lrd::AxisTables tab = P->tab;
   void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv, (void*)&rank, (void*)&wgt,
@@ -402,10 +438,14 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   }
   // brick shape
   int best[3] = {1, 1, 1};
-  choose_brick(dims, pat, corners, best);
+  int rsplit = 1, rtpt = 4;
+  if (pr->recon_split != 0 && pr->recon_split != 1 && pr->recon_split != 2 && pr->recon_split != 4)
+    return fail(LRD_ERR_INVALID, "recon_split must be 0, 1, 2 or 4, got %d", pr->recon_split);
+  pick_recon_layout(pr->nt, pr->recon_split, rsplit, rtpt);
+  choose_brick(dims, pat, corners, rsplit, best);
   if (pr->brick_x > 0 || pr->brick_y > 0 || pr->brick_z > 0) {
     if (pr->brick_x < 1 || pr->brick_y < 1 || pr->brick_z < 1 ||
-        (long long)pr->brick_x * pr->brick_y * pr->brick_z * lrd::kReconSplit > 1024)
+        (long long)pr->brick_x * pr->brick_y * pr->brick_z * rsplit > 1024)
       return fail(LRD_ERR_INVALID, "brick %dx%dx%d: each side >= 1 and at most 256 voxels", pr->brick_x,
                   pr->brick_y, pr->brick_z);
     best[0] = pr->brick_x;
@@ -474,7 +514,8 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   }
 
   const int T = pr->nt;
-  P->tpt = pick_tpt(T);
+  P->tpt = rtpt;
+  P->split = rsplit;
   const int nb4 = (T + 3) / 4;
   P->gram_threads = nb4 * (nb4 + 1) / 2;
   P->center_warps = 4;
@@ -501,8 +542,8 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
     P->refine_blocks = std::max(1, std::min<int>(2 * sms, (int)std::min<long long>(g.npatch, 1 << 20)));
   }
   if (!rc) rc = set_smem(eigh_kernel_for(T), P->smem_eigh);
-  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, false), P->smem_recon);
-  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, true), P->smem_recon);
+  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, false), P->smem_recon);
+  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, true), P->smem_recon);
   if (rc) {
     cudaFree(P->d_tables);
     delete P;

@@ -14,8 +14,9 @@
 // The result is deterministic and rounds like the step-0 loop, which adds the
 // patches to each voxel in exactly that order.
 //
-// Layout: one CTA per brick of bx*by*bz voxels, 4 threads per voxel (thread
-// ``s`` of a voxel owns the contiguous frames [s*TPT, s*TPT + TPT) ∩ [0, T)).
+// Layout: one CTA per brick of bx*by*bz voxels, SPLIT threads per voxel
+// (1, 2 or 4; thread ``s`` of a voxel owns the contiguous frames
+// [s*TPT, s*TPT + TPT) ∩ [0, T)).
 // The ranks and weights of every patch touching the brick are loaded once;
 // the CTA then walks those patches in x-major order with the eigenvector
 // block V_p (p x T, k-major, rows padded to a multiple of 4 floats) of the
@@ -36,7 +37,7 @@
 
 namespace lrd {
 
-constexpr int kReconSplit = 4;  // threads per voxel
+constexpr int kReconSplit = 4;  // largest number of threads per voxel
 
 __device__ __forceinline__ void two_sum_acc(float& acc, float& comp, float x) {
   const float s = __fadd_rn(acc, x);
@@ -65,8 +66,8 @@ __host__ __device__ inline size_t recon_smem_bytes(int T, int max_touch) {
   return sizeof(float) * 2 * (size_t)T * recon_tp(T) + (sizeof(int) + sizeof(float)) * (size_t)max_touch;
 }
 
-// grid: nbx*nby*nbz blocks of bx*by*bz*4 threads (<= 1024).
-template <int TPT, bool ACCURATE>
+// grid: nbx*nby*nbz blocks of bx*by*bz*SPLIT threads (<= 1024).
+template <int TPT, int SPLIT, bool ACCURATE>
 __global__ void recon_kernel(const float* __restrict__ xc, const float* __restrict__ mean,
                              const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
                              const float* __restrict__ wgt, float* __restrict__ out, Geom g,
@@ -79,8 +80,8 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
   int* s_rank = reinterpret_cast<int*>(sm_recon + 2 * (size_t)T * TP);
   const int tid = threadIdx.x;
   const int nthreads = blockDim.x;
-  const int slice = tid & (kReconSplit - 1);
-  const int vl = tid / kReconSplit;
+  const int slice = tid & (SPLIT - 1);
+  const int vl = tid / SPLIT;
   const int t0 = slice * TPT;
 
   int brick = blockIdx.x;
@@ -177,23 +178,31 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
 #pragma unroll
     for (int u = 0; u < TPT; ++u) xdp[u] = 0.f;
     for (int kk = 0; kk < p; ++kk) {
-      float v[TPT];
+      // v_k is read twice from shared memory rather than held in TPT registers
       const float4* vr = reinterpret_cast<const float4*>(vb + (size_t)kk * TP + t0);
-#pragma unroll
-      for (int u4 = 0; u4 < TPT / 4; ++u4) {
-        const float4 q = (t0 + 4 * u4 < TP) ? vr[u4] : make_float4(0.f, 0.f, 0.f, 0.f);
-        v[4 * u4 + 0] = q.x;
-        v[4 * u4 + 1] = q.y;
-        v[4 * u4 + 2] = q.z;
-        v[4 * u4 + 3] = q.w;
-      }
       float part = 0.f;
 #pragma unroll
-      for (int u = 0; u < TPT; ++u) part = fmaf(xr[u], v[u], part);
-      part += __shfl_xor_sync(0xffffffffu, part, 1);
-      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      for (int u4 = 0; u4 < TPT / 4; ++u4) {
+        if (t0 + 4 * u4 < TP) {
+          const float4 q = vr[u4];
+          part = fmaf(xr[4 * u4 + 0], q.x, part);
+          part = fmaf(xr[4 * u4 + 1], q.y, part);
+          part = fmaf(xr[4 * u4 + 2], q.z, part);
+          part = fmaf(xr[4 * u4 + 3], q.w, part);
+        }
+      }
+      if (SPLIT >= 2) part += __shfl_xor_sync(0xffffffffu, part, 1);
+      if (SPLIT >= 4) part += __shfl_xor_sync(0xffffffffu, part, 2);
 #pragma unroll
-      for (int u = 0; u < TPT; ++u) xdp[u] = fmaf(part, v[u], xdp[u]);
+      for (int u4 = 0; u4 < TPT / 4; ++u4) {
+        if (t0 + 4 * u4 < TP) {
+          const float4 q = vr[u4];
+          xdp[4 * u4 + 0] = fmaf(part, q.x, xdp[4 * u4 + 0]);
+          xdp[4 * u4 + 1] = fmaf(part, q.y, xdp[4 * u4 + 1]);
+          xdp[4 * u4 + 2] = fmaf(part, q.z, xdp[4 * u4 + 2]);
+          xdp[4 * u4 + 3] = fmaf(part, q.w, xdp[4 * u4 + 3]);
+        }
+      }
     }
     if (cov) {
       if (ACCURATE) {
