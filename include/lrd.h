@@ -164,6 +164,27 @@ int lrd_plan_phase_ms(lrd_plan* plan, float* ms /* LRD_NUM_PHASES */, int32_t* n
 int lrd_denoise_static(const lrd_problem* problem, const float* d_vol, float* d_out, int32_t* d_ranks,
                        void* stream);
 
+/* Batched form: many volumes of different shapes (frame counts, patch sizes,
+ * strides) in one call. Replaces a Python loop of the ladder's ``denoise``
+ * over volumes (step8_tuned.py:116-146 per volume).
+ *
+ * lrd_batch_plan_create builds one plan per problem (the problems' brick and
+ * split fields may carry autotuned values) and ``n_streams`` internal streams.
+ * lrd_batch_denoise forks from ``stream`` onto the internal streams (volume i
+ * on stream i mod n_streams, so small volumes overlap on the device), runs
+ * every volume's pipeline, joins back into ``stream``. d_vols, d_outs and
+ * d_ranks are host arrays of n device pointers (d_ranks and its entries may be
+ * NULL); the workspace is one allocation of lrd_batch_workspace_size bytes.
+ * With ``use_graph`` the whole batch is captured once into a CUDA graph and
+ * later calls with the same pointers replay it as a single graph launch
+ * (different pointers re-capture). No host synchronisation. */
+typedef struct lrd_batch_plan lrd_batch_plan;
+int lrd_batch_plan_create(const lrd_problem* problems, int32_t n, int32_t n_streams, lrd_batch_plan** plan);
+int lrd_batch_plan_destroy(lrd_batch_plan* plan);
+int lrd_batch_workspace_size(const lrd_batch_plan* plan, size_t* bytes);
+int lrd_batch_denoise(lrd_batch_plan* plan, const float* const* d_vols, float* const* d_outs,
+                      int32_t* const* d_ranks, void* d_workspace, void* stream, int32_t use_graph);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* lrd_last_error_string(void);
 int lrd_version(void);

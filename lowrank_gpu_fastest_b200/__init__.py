@@ -20,5 +20,12 @@ def denoise(*args, **kwargs):
     return _d(*args, **kwargs)
 
 
-__all__ = ["denoise", "Problem", "patch_corners", "patch_bases", "n_patches", "make_phantom",
+def denoise_batch(*args, **kwargs):
+    """See :func:`lowrank_gpu_fastest_b200.api.denoise_batch`."""
+    from .api import denoise_batch as _d
+
+    return _d(*args, **kwargs)
+
+
+__all__ = ["denoise", "denoise_batch", "Problem", "patch_corners", "patch_bases", "n_patches", "make_phantom",
            "make_phantom_lowrank", "rel_l2"]

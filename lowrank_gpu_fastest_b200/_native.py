@@ -41,6 +41,11 @@ SIGNATURES = {
     "lrd_plan_phase_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int32)]),
     "lrd_denoise_static": (ctypes.c_int, [ctypes.c_void_p] * 5),
+    "lrd_batch_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.POINTER(ctypes.c_void_p)]),
+    "lrd_batch_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "lrd_batch_workspace_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "lrd_batch_denoise": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int32]),
     "lrd_workspace_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.c_void_p]),
 }
@@ -154,3 +159,43 @@ class Plan:
 
     def stage_eigh(self, d_gram, d_lam, d_vecs, d_ranks, d_ws, stream):
         check(load().lrd_stage_eigh(self.handle, d_gram, d_lam, d_vecs, d_ranks, d_ws, stream))
+
+
+class BatchPlan:
+    """Owns an ``lrd_batch_plan*``: many problems, internal streams, a CUDA graph."""
+
+    def __init__(self, problems, n_streams=4):
+        """``problems``: list of dicts with shape, patch, stride, form, batch,
+        brick, split (the last four optional)."""
+        lib = load()
+        arr = (LrdProblem * len(problems))()
+        for i, pr in enumerate(problems):
+            nx, ny, nz, nt = (int(v) for v in pr["shape"])
+            px, py, pz = (int(v) for v in pr.get("patch", (11, 11, 11)))
+            bx, by, bz = (int(v) for v in (pr.get("brick") or (0, 0, 0)))
+            arr[i] = LrdProblem(nx, ny, nz, nt, px, py, pz, int(pr.get("stride", 3)),
+                                FORMS[pr.get("form", "plain")], int(pr.get("batch") or 0), bx, by, bz,
+                                int(pr.get("split") or 0))
+        self._arr = arr
+        self.n = len(problems)
+        h = ctypes.c_void_p()
+        check(lib.lrd_batch_plan_create(arr, self.n, int(n_streams), ctypes.byref(h)))
+        self.handle = h
+        ws = ctypes.c_size_t()
+        check(lib.lrd_batch_workspace_size(h, ctypes.byref(ws)))
+        self.workspace_bytes = int(ws.value)
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                load().lrd_batch_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    def denoise(self, d_vols, d_outs, d_ranks, d_ws, stream, use_graph=True):
+        vp = (ctypes.c_void_p * self.n)(*d_vols)
+        op = (ctypes.c_void_p * self.n)(*d_outs)
+        rp = (ctypes.c_void_p * self.n)(*d_ranks) if d_ranks is not None else None
+        check(load().lrd_batch_denoise(self.handle, vp, op, rp, d_ws, stream, int(bool(use_graph))))

@@ -119,3 +119,81 @@ def _denoise_host(t, patch, stride, batch, form, return_ranks, as_numpy):
         r = ranks.cpu()
         return res, (r.numpy() if as_numpy else r)
     return res
+
+
+_batch_plans: dict = {}
+
+
+def denoise_batch(vols, patches=(11, 11, 11), strides=3, *, form="plain", use_graph=True, n_streams=4,
+                  autotune=False, return_ranks=False):
+    """Denoise many 4D volumes of different shapes in one batched call.
+
+    ``vols``: list of float32 CUDA tensors (device-resident; outputs are CUDA
+    tensors) or numpy arrays (copied in and out). ``patches`` / ``strides``:
+    one value for all volumes or one per volume. Volume i runs on internal
+    stream i mod ``n_streams``; with ``use_graph`` the whole batch is one
+    CUDA-graph launch, captured on the first call with these buffers. With
+    ``autotune`` each distinct (frames, patch, stride) gets its reconstruction
+    launch shape from :func:`lowrank_gpu_fastest_b200.tune.tune`.
+    """
+    if not torch.cuda.is_available():
+        raise RuntimeError("denoise_batch needs a CUDA device")
+    n = len(vols)
+    if n == 0:
+        return ([], []) if return_ranks else []
+    if isinstance(patches, (list, tuple)) and len(patches) == n and isinstance(patches[0], (list, tuple)):
+        plist = [tuple(int(v) for v in p) for p in patches]
+    else:
+        plist = [tuple(int(v) for v in patches)] * n
+    slist = list(strides) if isinstance(strides, (list, tuple)) else [int(strides)] * n
+    host = not torch.is_tensor(vols[0]) or not vols[0].is_cuda
+    device = torch.cuda.current_device()
+    dev_vols = []
+    for v in vols:
+        if host:
+            t = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float32)) if isinstance(v, np.ndarray) else v
+            dev_vols.append(t.to(f"cuda:{device}", non_blocking=False).contiguous())
+        else:
+            if v.dtype != torch.float32 or v.dim() != 4:
+                raise ValueError("every volume must be a 4D float32 tensor")
+            dev_vols.append(v.contiguous())
+    problems = []
+    for v, p, s in zip(dev_vols, plist, slist):
+        pr = dict(shape=tuple(v.shape), patch=p, stride=int(s), form=form)
+        if autotune:
+            from .tune import tune
+
+            brick, split = tune(tuple(v.shape), p, int(s), form, device)
+            pr["brick"], pr["split"] = brick, split
+        problems.append(pr)
+    key = (device, int(n_streams), tuple((pr["shape"], pr["patch"], pr["stride"], pr["form"],
+                                          tuple(pr.get("brick") or ()), pr.get("split", 0)) for pr in problems))
+    with _lock:
+        bp = _batch_plans.get(key)
+        if bp is None:
+            bp = _native.BatchPlan(problems, n_streams)
+            _batch_plans[key] = bp
+            bp.buffers = None
+    if bp.buffers is None or any(o.shape != v.shape for o, v in zip(bp.buffers["outs"], dev_vols)):
+        bp.buffers = dict(
+            ws=torch.empty(max(bp.workspace_bytes, 1), dtype=torch.uint8, device=f"cuda:{device}"),
+            outs=[torch.empty_like(v) for v in dev_vols],
+            ranks=[torch.empty(_n_patches(pr), dtype=torch.int32, device=f"cuda:{device}") for pr in problems],
+        )
+    buf = bp.buffers
+    stream = torch.cuda.current_stream(device)
+    bp.denoise([v.data_ptr() for v in dev_vols], [o.data_ptr() for o in buf["outs"]],
+               [r.data_ptr() for r in buf["ranks"]], buf["ws"].data_ptr(), stream.cuda_stream, use_graph)
+    if host:
+        outs = [o.cpu().numpy() for o in buf["outs"]]
+        ranks = [r.cpu().numpy() for r in buf["ranks"]]
+    else:
+        outs = [o.clone() for o in buf["outs"]]
+        ranks = [r.clone() for r in buf["ranks"]]
+    return (outs, ranks) if return_ranks else outs
+
+
+def _n_patches(pr):
+    from .problem import n_patches
+
+    return n_patches(pr["shape"], pr["patch"], pr["stride"])

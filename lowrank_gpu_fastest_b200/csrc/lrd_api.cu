@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -91,14 +93,16 @@ namespace {
 
 // Reconstruction thread layout for T frames: two threads per voxel up to
 // T = 96 (one shuffle per eigenvector; one thread per voxel needs ~220
-// registers at T = 48 and measured 3.4x slower), four above; frames per
-// thread rounded up to a multiple of 4 (float4 reads of the eigenvectors).
+// registers at T = 48 and measured 3.4x slower), four above. The frames are
+// cut into four chunks of Q = round4(ceil(T/4)) and a thread owns 4/split
+// consecutive chunks (TPT = Q * 4 / split), so every split sums y_k in the
+// same tree.
 void pick_recon_layout(int T, int want_split, int& split, int& tpt) {
   split = T <= 96 ? 2 : 4;
   if (want_split == 1 || want_split == 2 || want_split == 4) split = std::max(want_split, split);
-  tpt = ((T + split - 1) / split + 3) & ~3;
-  if (split == 2) tpt = std::max(tpt, 12);
-  if (split == 4) tpt = std::max(tpt, 8);
+  if (T > 48 && split == 1) split = 2;
+  const int q = (((T + 3) / 4) + 3) & ~3;
+  tpt = q * 4 / split;
 }
 
 // Brick choice for the reconstruction: minimise the thread-slots the CTAs spend
@@ -187,34 +191,22 @@ void* recon_fn(bool accurate) {
 void* recon_kernel_ptr(int tpt, int split, bool accurate) {
   if (split == 1) {
     switch (tpt) {
-      case 4: return recon_fn<4, 1>(accurate);
-      case 8: return recon_fn<8, 1>(accurate);
-      case 12: return recon_fn<12, 1>(accurate);
       case 16: return recon_fn<16, 1>(accurate);
-      case 20: return recon_fn<20, 1>(accurate);
-      case 24: return recon_fn<24, 1>(accurate);
-      case 28: return recon_fn<28, 1>(accurate);
       case 32: return recon_fn<32, 1>(accurate);
-      case 36: return recon_fn<36, 1>(accurate);
-      case 40: return recon_fn<40, 1>(accurate);
-      case 44: return recon_fn<44, 1>(accurate);
       case 48: return recon_fn<48, 1>(accurate);
     }
   } else if (split == 2) {
     switch (tpt) {
-      case 12: return recon_fn<12, 2>(accurate);
+      case 8: return recon_fn<8, 2>(accurate);
       case 16: return recon_fn<16, 2>(accurate);
-      case 20: return recon_fn<20, 2>(accurate);
       case 24: return recon_fn<24, 2>(accurate);
-      case 28: return recon_fn<28, 2>(accurate);
       case 32: return recon_fn<32, 2>(accurate);
-      case 36: return recon_fn<36, 2>(accurate);
       case 40: return recon_fn<40, 2>(accurate);
-      case 44: return recon_fn<44, 2>(accurate);
       case 48: return recon_fn<48, 2>(accurate);
     }
   } else if (split == 4) {
     switch (tpt) {
+      case 4: return recon_fn<4, 4>(accurate);
       case 8: return recon_fn<8, 4>(accurate);
       case 12: return recon_fn<12, 4>(accurate);
       case 16: return recon_fn<16, 4>(accurate);
@@ -227,11 +219,23 @@ void* recon_kernel_ptr(int tpt, int split, bool accurate) {
   return nullptr;
 }
 
+// The dynamic shared-memory limit is a property of the kernel, shared by
+// every plan in the process: only ever raise it (per device and kernel), so a
+// plan created later with a smaller need cannot shrink an earlier plan's.
+std::mutex g_smem_mu;
+std::map<std::pair<int, const void*>, size_t> g_smem_set;
+
 int set_smem(const void* fn, size_t bytes) {
-  if (bytes > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(max dynamic smem)");
-  }
+  if (bytes <= 48 * 1024) return LRD_OK;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_smem_mu);
+  size_t& cur = g_smem_set[{dev, fn}];
+  if (bytes <= cur) return LRD_OK;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(max dynamic smem)");
+  cur = bytes;
   return LRD_OK;
 }
 
@@ -712,3 +716,4 @@ int lrd_stage_eigh(const lrd_plan* P, const float* d_gram, float* d_lam, float* 
 }  // extern "C"
 
 #include "lrd_static.inc"
+#include "lrd_batch.inc"

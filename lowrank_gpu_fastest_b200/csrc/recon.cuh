@@ -178,21 +178,38 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
 #pragma unroll
     for (int u = 0; u < TPT; ++u) xdp[u] = 0.f;
     for (int kk = 0; kk < p; ++kk) {
-      // v_k is read twice from shared memory rather than held in TPT registers
+      // v_k is read twice from shared memory rather than held in TPT registers.
+      // y_k = (x - m) . v_k is summed as four fixed frame chunks of TPT*SPLIT/4
+      // frames, combined ((c0 + c1) + (c2 + c3)), for every SPLIT, so the
+      // result does not depend on the thread layout.
       const float4* vr = reinterpret_cast<const float4*>(vb + (size_t)kk * TP + t0);
-      float part = 0.f;
+      constexpr int CH = 4 / SPLIT;         // chunks per thread
+      constexpr int CU4 = TPT / 4 / CH;     // float4 groups per chunk
+      float cp[CH];
 #pragma unroll
-      for (int u4 = 0; u4 < TPT / 4; ++u4) {
-        if (t0 + 4 * u4 < TP) {
-          const float4 q = vr[u4];
-          part = fmaf(xr[4 * u4 + 0], q.x, part);
-          part = fmaf(xr[4 * u4 + 1], q.y, part);
-          part = fmaf(xr[4 * u4 + 2], q.z, part);
-          part = fmaf(xr[4 * u4 + 3], q.w, part);
+      for (int c = 0; c < CH; ++c) {
+        float acc_c = 0.f;
+#pragma unroll
+        for (int u4 = c * CU4; u4 < (c + 1) * CU4; ++u4) {
+          if (t0 + 4 * u4 < TP) {
+            const float4 q = vr[u4];
+            acc_c = fmaf(xr[4 * u4 + 0], q.x, acc_c);
+            acc_c = fmaf(xr[4 * u4 + 1], q.y, acc_c);
+            acc_c = fmaf(xr[4 * u4 + 2], q.z, acc_c);
+            acc_c = fmaf(xr[4 * u4 + 3], q.w, acc_c);
+          }
         }
+        cp[c] = acc_c;
       }
-      if (SPLIT >= 2) part += __shfl_xor_sync(0xffffffffu, part, 1);
-      if (SPLIT >= 4) part += __shfl_xor_sync(0xffffffffu, part, 2);
+      float part;
+      if (CH == 4)
+        part = __fadd_rn(__fadd_rn(cp[0], cp[CH > 1 ? 1 : 0]), __fadd_rn(cp[CH > 2 ? 2 : 0], cp[CH > 3 ? 3 : 0]));
+      else if (CH == 2)
+        part = __fadd_rn(cp[0], cp[CH > 1 ? 1 : 0]);
+      else
+        part = cp[0];
+      if (SPLIT >= 2) part = __fadd_rn(part, __shfl_xor_sync(0xffffffffu, part, 1));
+      if (SPLIT >= 4) part = __fadd_rn(part, __shfl_xor_sync(0xffffffffu, part, 2));
 #pragma unroll
       for (int u4 = 0; u4 < TPT / 4; ++u4) {
         if (t0 + 4 * u4 < TP) {
