@@ -52,7 +52,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--form", choices=["plain", "accurate"], default="plain")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="headline")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="headline")
+    ap.add_argument("--volumes", type=int, default=24, help="batched: number of volumes")
+    ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (req/s)")
+    ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="patches in the CPU sample (0 = auto)")
     ap.add_argument("--brick", default=None, help="recon brick bx,by,bz (default: the plan's choice)")
@@ -415,8 +419,103 @@ def run_ours(args, wl):
         dist.destroy_process_group()
 
 
+def run_batched(args):
+    """Batched uneven form: ``--volumes`` seeded volumes of mixed shapes in one
+    CUDA-graph launch per step (device-timed)."""
+    import torch
+
+    from lowrank_gpu_fastest_b200 import api
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+    from lowrank_gpu_fastest_b200.problem import n_patches
+    from lowrank_gpu_fastest_b200.serve import draw_request_shapes
+
+    shapes = draw_request_shapes(args.volumes, seed=args.seed, big_fraction=0.0)
+    vols = [torch.from_numpy(make_phantom_lowrank(r["shape"], seed=i, sigma=r["sigma"])[0]).cuda()
+            for i, r in enumerate(shapes)]
+    patches = [r["patch"] for r in shapes]
+    strides = [r["stride"] for r in shapes]
+    P = sum(n_patches(r["shape"], r["patch"], r["stride"]) for r in shapes)
+    for _ in range(args.warmup):
+        api.denoise_batch(vols, patches, strides, use_graph=True)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        api.denoise_batch(vols, patches, strides, use_graph=True)
+        e.record()
+        torch.cuda.synchronize()
+        times.append(s.elapsed_time(e))
+    ms = statistics.mean(times)
+    N = [int(np.prod(r["patch"])) for r in shapes]
+    flops = sum(4 * n * r["shape"][3] ** 2 * n_patches(r["shape"], r["patch"], r["stride"]) for n, r in zip(N, shapes))
+    print(json.dumps(dict(
+        metric="patches_per_s", workload="batched", value=P / (ms * 1e-3), unit="patches/s", n_gpus=1,
+        steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, dtype="f32", data="synthetic",
+        config=dict(volumes=args.volumes, seed=args.seed, patches=P, algorithmic_tflop=flops / 1e12,
+                    shapes=[[list(r["shape"]), r["patch"][0], r["stride"]] for r in shapes],
+                    note="one lrd_batch_denoise CUDA-graph launch per step, volumes on 4 internal streams"),
+        achieved_tflops=flops / (ms * 1e-3) / 1e12)), flush=True)
+
+
+def run_serving(args):
+    """Serving form: ``--requests`` seeded requests arriving as a Poisson
+    stream at ``--rate`` req/s (10% 128x128x64x96 / 11^3 / stride 2), served
+    with continuous batching; compared with solving the same requests one
+    after another."""
+    import torch
+
+    from lowrank_gpu_fastest_b200 import api
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+    from lowrank_gpu_fastest_b200.serve import Server, draw_request_shapes, poisson_arrivals
+
+    shapes = draw_request_shapes(args.requests, seed=args.seed, big_fraction=0.1)
+    arr = poisson_arrivals(args.rate, 1e9, seed=args.seed)[: args.requests]
+    vols = [make_phantom_lowrank(r["shape"], seed=i, sigma=r["sigma"])[0] for i, r in enumerate(shapes)]
+    # warm: plans and one solve per distinct problem
+    seen = set()
+    for v, r in zip(vols, shapes):
+        k = (v.shape, r["patch"], r["stride"])
+        if k not in seen:
+            seen.add(k)
+            api.denoise(torch.from_numpy(v).cuda(), r["patch"], r["stride"])
+    torch.cuda.synchronize()
+    # sequential plain-form solves (host -> host each)
+    t0 = time.perf_counter()
+    for v, r in zip(vols, shapes):
+        api.denoise(v, r["patch"], r["stride"])
+    seq_s = time.perf_counter() - t0
+    from lowrank_gpu_fastest_b200.problem import n_patches
+
+    P = sum(n_patches(v.shape, r["patch"], r["stride"]) for v, r in zip(vols, shapes))
+    with Server(n_slots=4) as srv:
+        start = time.perf_counter()
+        futs = []
+        for t, v, r in zip(arr, vols, shapes):
+            now = time.perf_counter() - start
+            if t > now:
+                time.sleep(t - now)
+            futs.append(srv.submit(v, r["patch"], r["stride"]))
+        for f in futs:
+            f.result()
+        st = srv.stats()
+    print(json.dumps(dict(
+        metric="patches_per_s", workload="serving", value=st["patches_per_s"], unit="patches/s", n_gpus=1,
+        higher_is_better=True, dtype="f32", data="synthetic",
+        p50_ms=st["p50_ms"], p99_ms=st["p99_ms"], mean_ms=st["mean_ms"], requests=st["n"],
+        requests_per_s=st["requests_per_s"], sequential_patches_per_s=P / seq_s,
+        vs_sequential=st["patches_per_s"] / (P / seq_s),
+        config=dict(requests=args.requests, rate_per_s=args.rate, seed=args.seed, slots=4,
+                    mix="x,y 64..128, z 32..64, T {32,48,64,96}, patch {5,7,11}^3, stride {1,2,3}; "
+                        "10% 128x128x64x96 / 11^3 / stride 2"))), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "serving":
+        return run_serving(args)
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)

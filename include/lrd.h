@@ -41,6 +41,7 @@ enum lrd_status {
 
 /* Bits of the device status word (lrd_workspace_status). */
 #define LRD_STATUS_TMA_TIMEOUT 1 /* a TMA completion wait exceeded its deadline */
+#define LRD_STATUS_MMA_TIMEOUT 2 /* a tensor-core completion wait exceeded its deadline */
 
 /* Arithmetic forms of the path. */
 enum lrd_form {
@@ -51,7 +52,13 @@ enum lrd_form {
   /* Same contractions; the accumulation keeps the temporal mean out of the
    * running sums (out = m + sum w (x-m)P / sum w, float64 weight sums): error
    * against a float64 run of the algorithm at the float32 output floor. */
-  LRD_FORM_ACCURATE = 1
+  LRD_FORM_ACCURATE = 1,
+  /* Precision form: the Gram contraction on the tcgen05 tensor cores in TF32
+   * with 3xTF32 split products (x = hi + lo; hi.hi + hi.lo + lo.hi) and FP32
+   * accumulation in tensor memory (T <= 64, px*py <= 128; otherwise the FP32
+   * Gram), near-tie MP decisions redone in FP64, the accurate form's
+   * accumulation. */
+  LRD_FORM_TENSOR = 2
 };
 
 /* One problem: volume (nx, ny, nz, nt), patch (px, py, pz), one stride for the

@@ -46,8 +46,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the phase with parity ``parity`` to complete.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int* status) {
+// Bounded wait for the phase with parity ``parity`` to complete; on expiry
+// ``code`` is or-ed into the status word.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int* status,
+                                                  int code = kStatusTmaTimeout) {
   const unsigned long long t0 = globaltimer_ns();
   for (;;) {
     uint32_t ok;
@@ -58,7 +60,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
         : "memory");
     if (ok) return true;
     if (globaltimer_ns() - t0 > kWaitNs) {
-      atomicOr(status, kStatusTmaTimeout);
+      atomicOr(status, code);
       return false;
     }
   }

@@ -18,6 +18,7 @@
 #include "eigh.cuh"
 #include "eigh_reg.cuh"
 #include "gram.cuh"
+#include "gram_tc.cuh"
 #include "gram_z.cuh"
 #include "lrd_common.cuh"
 #include "recon.cuh"
@@ -68,6 +69,8 @@ struct lrd_plan {
   int split;               // recon threads per voxel
   int gram_threads;
   bool use_gramz;          // column Gram kernel (TMA-staged z-planes) instead of per-patch
+  bool use_gramtc;         // the column Gram on tcgen05 (tensor form)
+  size_t smem_gramtc;
   int gramz_ring;          // window accumulator slots
   size_t smem_gramz;
   size_t smem_center, smem_gram, smem_eigh, smem_recon;
@@ -289,7 +292,7 @@ int encode_plane_map(const lrd_plan* P, const float* xc, CUtensorMap* map) {
 
 int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
-  if (P->use_gramz) {
+  if (P->use_gramz || P->use_gramtc) {
     CUtensorMap map;
     int rc = encode_plane_map(P, xc, &map);
     if (rc) return rc;
@@ -299,9 +302,15 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
     const long long TT = (long long)P->g.nt * P->g.nt;
     for (long long c0 = 0; c0 < ncol; c0 += cols) {
       const long long nc = std::min(cols, ncol - c0);
-      lrd::gram_z_kernel<<<(unsigned)nc, P->gram_threads, P->smem_gramz, st>>>(
-          map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, status);
-      rc = launch_check("gram_z_kernel launch");
+      if (P->use_gramtc) {
+        lrd::gram_tc_kernel<<<(unsigned)nc, 128, P->smem_gramtc, st>>>(map, d_gram + c0 * P->g.ncz * TT, P->g,
+                                                                      P->tab, c0, P->gramz_ring, status);
+        rc = launch_check("gram_tc_kernel launch");
+      } else {
+        lrd::gram_z_kernel<<<(unsigned)nc, P->gram_threads, P->smem_gramz, st>>>(
+            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, status);
+        rc = launch_check("gram_z_kernel launch");
+      }
       if (rc) return rc;
     }
     return LRD_OK;
@@ -363,7 +372,7 @@ int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st) {
   const float* gv = reinterpret_cast<const float*>(ws + P->off_gv);
   const int32_t* rank = reinterpret_cast<const int32_t*>(ws + P->off_rank);
   const float* wgt = reinterpret_cast<const float*>(ws + P->off_wgt);
-  const bool acc = P->prob.form == LRD_FORM_ACCURATE;
+  const bool acc = P->prob.form != LRD_FORM_PLAIN;
   const unsigned nbricks = (unsigned)((long long)P->g.nbx * P->g.nby * P->g.nbz);
   const unsigned threads = (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
   void* fn = recon_kernel_ptr(P->tpt, P->split, acc);
@@ -408,7 +417,7 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   if (pr->nt < 2) return fail(LRD_ERR_INVALID, "need at least 2 frames, got %d", pr->nt);
   if (pr->nt > lrd::kMaxT) return fail(LRD_ERR_UNSUPPORTED, "nt=%d exceeds the compiled limit %d", pr->nt, lrd::kMaxT);
   if (pr->stride < 1) return fail(LRD_ERR_INVALID, "stride must be >= 1, got %d", pr->stride);
-  if (pr->form != LRD_FORM_PLAIN && pr->form != LRD_FORM_ACCURATE)
+  if (pr->form != LRD_FORM_PLAIN && pr->form != LRD_FORM_ACCURATE && pr->form != LRD_FORM_TENSOR)
     return fail(LRD_ERR_INVALID, "unknown form %d", pr->form);
   if (pr->batch < 0) return fail(LRD_ERR_INVALID, "batch must be >= 0, got %d", pr->batch);
   const long long nvox = (long long)pr->nx * pr->ny * pr->nz;
@@ -534,10 +543,14 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
     P->smem_gramz = lrd::gramz_smem_bytes(pr->px * pr->py, T, ring, P->gram_threads);
     P->use_gramz = (T % 4 == 0) && P->smem_gramz <= 200 * 1024 && tensor_map_encoder() != nullptr &&
                    pr->px <= 256 && pr->py <= 256;
+    P->smem_gramtc = lrd::gramtc_smem_bytes(pr->px * pr->py, T, ring);
+    P->use_gramtc = pr->form == LRD_FORM_TENSOR && T <= 64 && (T % 4 == 0) && pr->px * pr->py <= 128 &&
+                    P->smem_gramtc <= 220 * 1024 && tensor_map_encoder() != nullptr;
   }
   int rc = set_smem((const void*)lrd::center_kernel, P->smem_center);
   if (!rc) rc = set_smem((const void*)lrd::gram_kernel, P->smem_gram);
   if (!rc && P->use_gramz) rc = set_smem((const void*)lrd::gram_z_kernel, P->smem_gramz);
+  if (!rc && P->use_gramtc) rc = set_smem((const void*)lrd::gram_tc_kernel, P->smem_gramtc);
   P->smem_refine = lrd::eigh_refine_smem_bytes(T, pr->pz);
   if (!rc) rc = set_smem((const void*)lrd::eigh_refine_kernel, P->smem_refine);
   {

@@ -36,11 +36,12 @@ def test_small_plain_vs_step0(cuda_ok, name):
     assert rel_l2(out, g["out"]) <= PLAIN_TOL
 
 
+@pytest.mark.parametrize("form", ["accurate", "tensor"])
 @pytest.mark.parametrize("name", SMALL_CASES)
-def test_small_accurate_vs_fp64(cuda_ok, name):
+def test_small_accurate_vs_fp64(cuda_ok, name, form):
     g = load_golden(name)
     vol = golden_input(g)
-    out, ranks = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form="accurate")
+    out, ranks = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form=form)
     np.testing.assert_array_equal(ranks, g["ranks"])
     idx = g["sample_idx"]
     assert rel_l2(out.reshape(-1)[idx], g["out64_sample"]) <= ACCURATE_TOL
@@ -54,8 +55,10 @@ def test_large_ranks_and_sample(cuda_ok, name):
     np.testing.assert_array_equal(ranks, g["ranks"])
     idx = g["sample_idx"]
     assert rel_l2(out.reshape(-1)[idx], g["out_sample"]) <= PLAIN_TOL
-    outa, _ = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form="accurate")
-    assert rel_l2(outa.reshape(-1)[idx], g["out64_sample"]) <= ACCURATE_TOL_LARGE
+    for form in ("accurate", "tensor"):
+        outa, ra = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form=form)
+        np.testing.assert_array_equal(ra, g["ranks"])
+        assert rel_l2(outa.reshape(-1)[idx], g["out64_sample"]) <= ACCURATE_TOL_LARGE
 
 
 def test_config1_full_volume_vs_live_oracle(cuda_ok):
@@ -155,3 +158,40 @@ def test_stage_gram_and_eigh_vs_fp64_oracle(cuda_ok):
 def test_error_is_raised_for_bad_shapes(cuda_ok):
     with pytest.raises(_native.LrdError):
         api.denoise(torch.zeros(4, 4, 4, 8, device="cuda"), (5, 5, 5), 2)
+
+
+@pytest.mark.parametrize("name", ["lowrank_p5s2", "ref_small", "lowrank_t64", "aniso"])
+def test_tensor_core_gram_vs_fp64(cuda_ok, name):
+    """The tcgen05 3xTF32 Gram (tensor form) against float64 Grams of the
+    same centred patches: within 4e-6 of the largest entry (FP32 FFMA: ~1e-6)."""
+    g = load_golden(name)
+    vol = golden_input(g)
+    shape, patch, stride = vol.shape, tuple(int(v) for v in g["patch"]), int(g["stride"])
+    plan = api.get_plan(shape, patch, stride, form="tensor")
+    T, P = shape[3], plan.n_patches
+    d = torch.from_numpy(vol).cuda()
+    ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device="cuda")
+    gram = torch.empty(P, T, T, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    plan.stage_gram(d.data_ptr(), gram.data_ptr(), ws.data_ptr(), s)
+    assert plan.status(ws.data_ptr(), s) == 0
+    gram = gram.cpu().numpy()
+    corners = orc.patch_corners(shape, patch, stride)
+    for idx in range(0, P, max(1, P // 25)):
+        i, j, k = corners[idx]
+        x = vol[i:i + patch[0], j:j + patch[1], k:k + patch[2]].reshape(-1, T).astype(np.float64)
+        xc = x - x.mean(1, keepdims=True)
+        G = xc.T @ xc
+        assert np.abs(gram[idx] - G).max() <= 4e-6 * np.abs(G).max()
+
+
+def test_status_word_clear_after_runs(cuda_ok):
+    g = load_golden("ref_small")
+    vol = torch.from_numpy(golden_input(g)).cuda()
+    for form in ("plain", "tensor"):
+        plan = api.get_plan(tuple(vol.shape), (11, 11, 11), 3, form=form)
+        ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device="cuda")
+        out = torch.empty_like(vol)
+        s = torch.cuda.current_stream().cuda_stream
+        plan.denoise(vol.data_ptr(), out.data_ptr(), None, ws.data_ptr(), s)
+        assert plan.status(ws.data_ptr(), s) == 0
