@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["plain", "accurate"], default="plain")
+    ap.add_argument("--form", choices=["plain", "accurate", "tensor"], default="plain")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="headline")
     ap.add_argument("--volumes", type=int, default=24, help="batched: number of volumes")
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")

@@ -55,9 +55,9 @@ enum lrd_form {
   LRD_FORM_ACCURATE = 1,
   /* Precision form: the Gram contraction on the tcgen05 tensor cores in TF32
    * with 3xTF32 split products (x = hi + lo; hi.hi + hi.lo + lo.hi) and FP32
-   * accumulation in tensor memory (T <= 64, px*py <= 128; otherwise the FP32
-   * Gram), near-tie MP decisions redone in FP64, the accurate form's
-   * accumulation. */
+   * accumulation in tensor memory per plane (T <= 64, px*py <= 128; otherwise
+   * the FP32 Gram), near-tie MP decisions redone in FP64, the accurate
+   * form's accumulation. */
   LRD_FORM_TENSOR = 2
 };
 

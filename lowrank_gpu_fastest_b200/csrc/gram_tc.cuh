@@ -8,15 +8,19 @@
 //     H = hi^T hi + hi^T lo + lo^T hi        (3xTF32, FP32 accumulation in TMEM)
 // which recovers ~22 bits of each product.
 //
-// MMA shape: M = 128 (rows = frames t; rows >= T are never read back), N = T
-// (rounded up to 16), K = 8 voxels per instruction over the plane's voxels
+// MMA shape: M = 64 (rows = frames t; rows >= T are never read back), N = T
+// (rounded up to 8), K = 8 voxels per instruction over the plane's voxels
 // padded to a multiple of 8. A (M x K) and B (stored as its K-major transpose,
 // N x K) are the same shared-memory tile X^T in the canonical K-major,
 // no-swizzle layout: 8-row x 16-byte core matrices, LBO = 128 B between core
-// matrices along K, SBO = (K/4) * 128 B between 8-row groups. The
-// accumulator D (row i in TMEM lane i, column j in TMEM column j) is read back
-// by the four warps (warp w owns lanes 32w..32w+31) with tcgen05.ld, and
-// thread t (< T) adds row t of H into its windows' rows in shared memory.
+// matrices along K, SBO = (K/4) * 128 B between 8-row groups.
+//
+// Each plane's H is accumulated in tensor memory over its own 3 x K/8 MMAs
+// only (accumulating whole windows there - ~500 MMA steps - measured a 10x
+// larger Gram error: the tensor-core FP32 accumulation does not round to
+// nearest), read back with tcgen05.ld (M = 64: rows 16w..16w+15 in lanes
+// 32w..32w+15 of warp w's sub-partition) and added in float32 into the
+// windows' rows in shared memory; a completed window is written out.
 //
 // Waits (TMA and MMA completion) are bounded by %globaltimer deadlines; the
 // TMEM allocation is released on every path.
@@ -76,23 +80,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // Shared-memory layout (bytes): hi tile (ceil(T/8) row groups of SBO bytes),
-// lo tile (same), two plane slots, windows, mbarriers, TMEM address. An A
-// descriptor spans 16 row groups from its tile's start (M = 128); the rows
-// past T read whatever follows (they only feed accumulator rows >= T, which
-// are never read), so the allocation just has to cover lo + 16 groups.
+// lo tile (same), one plane slot, windows [ring][T cols][T rows] float32,
+// mbarriers, TMEM address, abort flag. An A descriptor spans 8 row groups
+// from its tile's start (M = 64); rows past T read whatever follows (they
+// only feed accumulator rows >= T, never read), so the allocation just has to
+// cover lo + 8 groups.
 __host__ __device__ inline int gramtc_kpad(int rows) { return (rows + 7) & ~7; }
 __host__ __device__ inline size_t gramtc_sbo(int rows) { return (size_t)(gramtc_kpad(rows) / 4) * 128; }
 __host__ __device__ inline size_t gramtc_tile_bytes(int rows, int T) { return (size_t)((T + 7) / 8) * gramtc_sbo(rows); }
-__host__ __device__ inline size_t gramtc_off_planes(int rows, int T) { return 2 * gramtc_tile_bytes(rows, T); }
+__host__ __device__ inline size_t gramtc_off_plane(int rows, int T) { return 2 * gramtc_tile_bytes(rows, T); }
 __host__ __device__ inline size_t gramtc_smem_bytes(int rows, int T, int ring) {
-  const size_t end = gramtc_off_planes(rows, T) +
-                     sizeof(float) * (2 * gramz_plane_floats(rows, T) + (size_t)ring * T * T) + 64;
-  const size_t span = gramtc_tile_bytes(rows, T) + 16 * gramtc_sbo(rows);
+  const size_t end = gramtc_off_plane(rows, T) +
+                     sizeof(float) * (gramz_plane_floats(rows, T) + (size_t)ring * T * T) + 64;
+  const size_t span = gramtc_tile_bytes(rows, T) + 8 * gramtc_sbo(rows);
   return end > span ? end : span;
 }
-// (+ 64 bytes at the end hold the three mbarriers, the TMEM address and the abort flag)
+__host__ __device__ inline int gramtc_npad(int T) { return (T + 7) & ~7; }
+__host__ __device__ inline int gramtc_tmem_cols(int T) { return gramtc_npad(T) <= 32 ? 32 : 64; }
 
-// grid: (columns in this launch); block: 128 threads (4 warps). T <= 64 and
+// grid: (columns in this launch); block: 128 threads (4 warps). T <= 64,
 // px*py <= 128. ``gram`` points at the Gram block of patch col0 * ncz.
 __global__ void __launch_bounds__(128)
     gram_tc_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g, AxisTables tab,
@@ -105,15 +111,13 @@ __global__ void __launch_bounds__(128)
   const size_t tile = gramtc_tile_bytes(rows, T);
   unsigned char* hi = smt;
   unsigned char* lo = smt + tile;
-  float* plane0 = reinterpret_cast<float*>(smt + gramtc_off_planes(rows, T));
-  float* plane1 = plane0 + gramz_plane_floats(rows, T);
-  float* win = plane1 + gramz_plane_floats(rows, T);  // [ring][T cols][T rows]
+  float* plane = reinterpret_cast<float*>(smt + gramtc_off_plane(rows, T));
+  float* win = plane + gramz_plane_floats(rows, T);  // [ring][T cols][T rows]
   uint64_t* bars = reinterpret_cast<uint64_t*>(win + (size_t)ring * T * T);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);  // set when a wait gave up
-  const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&bars[0]);
-  const uint32_t bar1 = (uint32_t)__cvta_generic_to_shared(&bars[1]);
-  const uint32_t barm = (uint32_t)__cvta_generic_to_shared(&bars[2]);
+  const uint32_t bart = (uint32_t)__cvta_generic_to_shared(&bars[0]);
+  const uint32_t barm = (uint32_t)__cvta_generic_to_shared(&bars[1]);
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
 
@@ -121,17 +125,17 @@ __global__ void __launch_bounds__(128)
   const int ci = (int)(col / g.ncy), cj = (int)(col % g.ncy);
   const int cx = tab.corners[0][ci], cy = tab.corners[1][cj];
   const uint32_t plane_bytes = (uint32_t)(rows * T * sizeof(float));
-  const int Npad = (T + 15) & ~15;
-  const uint32_t idesc = umma_idesc_tf32(128, Npad);
-  const uint32_t ncols = Npad <= 32 ? 32 : (Npad <= 64 ? 64 : 128);
+  const int Npad = gramtc_npad(T);
+  const uint32_t idesc = umma_idesc_tf32(64, Npad);
+  const uint32_t ncols = (uint32_t)gramtc_tmem_cols(T);
+  const int nv4 = (rows + 3) >> 2;
 
   // zero the operand tiles once (rows >= T and voxels >= rows stay zero) and the windows
   for (size_t e = tid; e < 2 * tile / 16; e += blockDim.x) reinterpret_cast<uint4*>(smt)[e] = make_uint4(0, 0, 0, 0);
   for (int e = tid; e < ring * T * T; e += blockDim.x) win[e] = 0.f;
   if (tid == 0) {
     *abort_flag = 0;
-    mbar_init(bar0, 1);
-    mbar_init(bar1, 1);
+    mbar_init(bart, 1);
     mbar_init(barm, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -148,41 +152,48 @@ __global__ void __launch_bounds__(128)
   const uint32_t tmem = *tmem_slot;
   const uint32_t hi_addr = (uint32_t)__cvta_generic_to_shared(hi);
   const uint32_t lo_addr = (uint32_t)__cvta_generic_to_shared(lo);
+  const uint32_t plane_addr = (uint32_t)__cvta_generic_to_shared(plane);
 
   if (tid == 0 && g.nz > 0) {
-    mbar_expect_tx(bar0, plane_bytes);
-    tma_load_4d((uint32_t)__cvta_generic_to_shared(plane0), &xmap, bar0, 0, 0, cy, cx);
+    mbar_expect_tx(bart, plane_bytes);
+    tma_load_4d(plane_addr, &xmap, bart, 0, 0, cy, cx);
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
   uint32_t mma_phase = 0;
+  // the row of H (and of the windows) this thread owns: t = 16*warp + lane, lanes 0..15
+  const int trow = warp * 16 + lane;
+  const bool owner = lane < 16 && trow < T;
   for (int z = 0; z < g.nz; ++z) {
     if (*abort_flag) break;  // uniform: read after the barrier closing the previous plane
-    const int slot = z & 1;
-    if (tid == 0 && z + 1 < g.nz) {
-      const uint32_t nb_ = slot ? bar0 : bar1;
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      mbar_expect_tx(nb_, plane_bytes);
-      tma_load_4d((uint32_t)__cvta_generic_to_shared(slot ? plane0 : plane1), &xmap, nb_, 0, z + 1, cy, cx);
-    }
-    if (!mbar_wait_bounded(slot ? bar1 : bar0, (uint32_t)((z >> 1) & 1), status)) *abort_flag = 1;
+    if (!mbar_wait_bounded(bart, (uint32_t)(z & 1), status)) *abort_flag = 1;
     const int klo = tab.cover[2][2 * z], khi = tab.cover[2][2 * z + 1];
-    if (klo <= khi) {  // uniform
-      // split the plane into the hi / lo K-major tiles: element (t, v) at
-      // (t/8)*SBO + (v/4)*128 + (t%8)*16 + (v%4)*4
-      const float* pl = slot ? plane1 : plane0;
-      for (int e = tid; e < rows * T; e += blockDim.x) {
-        const int v = e / T, t = e - v * T;
-        const float x = pl[e];
-        const uint32_t h = tf32_rna(x);
-        const uint32_t l = tf32_rna(x - __uint_as_float(h));
-        const uint32_t off = (uint32_t)(t >> 3) * sbo + (uint32_t)(v >> 2) * 128 + (uint32_t)(t & 7) * 16 +
-                             (uint32_t)(v & 3) * 4;
-        *reinterpret_cast<uint32_t*>(hi + off) = h;
-        *reinterpret_cast<uint32_t*>(lo + off) = l;
+    const bool active = klo <= khi;  // uniform
+    if (active) {
+      // split into the hi / lo K-major tiles; item (t, 4 voxels) -> one 16-byte
+      // core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16
+      for (int e = tid; e < T * nv4; e += blockDim.x) {
+        const int v4 = e / T, t = e - v4 * T;
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int v = 4 * v4 + i;
+          const float x = v < rows ? plane[v * T + t] : 0.f;
+          h[i] = tf32_rna(x);
+          l[i] = tf32_rna(x - __uint_as_float(h[i]));
+        }
+        const uint32_t off = (uint32_t)(t >> 3) * sbo + (uint32_t)v4 * 128 + (uint32_t)(t & 7) * 16;
+        *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
       }
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      __syncthreads();
-      if (tid == 0) {
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();  // tiles written, plane slot free
+    if (tid == 0) {
+      if (z + 1 < g.nz) {  // next plane streams in while this one's MMAs run
+        mbar_expect_tx(bart, plane_bytes);
+        tma_load_4d(plane_addr, &xmap, bart, 0, z + 1, cy, cx);
+      }
+      if (active) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         uint32_t acc = 0;
         for (int ks = 0; ks < kpad / 8; ++ks) {
@@ -196,29 +207,29 @@ __global__ void __launch_bounds__(128)
         }
         umma_commit(barm);
       }
+    }
+    if (active) {
       if (!mbar_wait_bounded(barm, mma_phase, status, kStatusMmaTimeout)) *abort_flag = 1;
       mma_phase ^= 1;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      // row t = 32*warp + lane of H; all lanes of a warp take part in tcgen05.ld
-      const int t = warp * 32 + lane;
-      if (warp * 32 < T) {
+      if (warp * 16 < T) {
         for (int c0 = 0; c0 < Npad; c0 += 16) {
           float h[16];
           tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, h);
-          if (t < T) {
+          if (owner) {
             for (int k = klo; k <= khi; ++k) {
-              float* w = win + (size_t)(k % ring) * T * T;
+              float* w = win + (size_t)(k % ring) * T * T + trow;  // column c at w[c * T]
               const bool last = z == tab.corners[2][k] + g.pz - 1;
-              float* G = G0 + (size_t)k * T * T;
+              float* G = G0 + (size_t)k * T * T + (size_t)trow * T;
 #pragma unroll
               for (int c = 0; c < 16; ++c) {
                 if (c0 + c < T) {
-                  const float val = w[(size_t)(c0 + c) * T + t] + h[c];
+                  const float val = w[(size_t)(c0 + c) * T] + h[c];
                   if (last) {
-                    G[(size_t)t * T + c0 + c] = val;
-                    w[(size_t)(c0 + c) * T + t] = 0.f;
+                    G[c0 + c] = val;
+                    w[(size_t)(c0 + c) * T] = 0.f;
                   } else {
-                    w[(size_t)(c0 + c) * T + t] = val;
+                    w[(size_t)(c0 + c) * T] = val;
                   }
                 }
               }
@@ -228,7 +239,7 @@ __global__ void __launch_bounds__(128)
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     }
-    __syncthreads();  // plane slot reuse, tiles and TMEM rewritten next plane
+    __syncthreads();  // TMEM and tiles rewritten next plane
   }
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols) : "memory");

@@ -545,7 +545,7 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
                    pr->px <= 256 && pr->py <= 256;
     P->smem_gramtc = lrd::gramtc_smem_bytes(pr->px * pr->py, T, ring);
     P->use_gramtc = pr->form == LRD_FORM_TENSOR && T <= 64 && (T % 4 == 0) && pr->px * pr->py <= 128 &&
-                    P->smem_gramtc <= 220 * 1024 && tensor_map_encoder() != nullptr;
+                    P->smem_gramtc <= 200 * 1024 && tensor_map_encoder() != nullptr;
   }
   int rc = set_smem((const void*)lrd::center_kernel, P->smem_center);
   if (!rc) rc = set_smem((const void*)lrd::gram_kernel, P->smem_gram);
