@@ -108,9 +108,13 @@ int lrd_denoise(const lrd_plan* plan, const float* d_vol, float* d_out, int32_t*
 
 /* Host-buffer form of lrd_denoise: copies ``h_vol`` (pinned or pageable host
  * memory) to ``d_in``, denoises into ``d_out``, copies the result to
- * ``h_out`` and waits for the stream. ``d_in``/``d_out`` are caller-owned
- * device buffers of the volume's size. This is the whole host->host call of
- * step8_tuned.py:116-146 (from_numpy().cuda() ... host.copy_(...)). */
+ * ``h_out`` and waits. ``d_in``/``d_out`` are caller-owned device buffers of
+ * the volume's size. This is the whole host->host call of step8_tuned.py:
+ * 116-146 (from_numpy().cuda() ... host.copy_(...)), pipelined: the volume
+ * moves in x-slabs on the plan's two copy streams, each slab's compute runs
+ * on ``stream`` as soon as its planes are in, and finished output planes copy
+ * out while later slabs compute (pinned host buffers make the copies
+ * asynchronous). Results are identical to lrd_denoise's. */
 int lrd_denoise_host(const lrd_plan* plan, const float* h_vol, float* h_out, int32_t* h_ranks,
                      float* d_in, float* d_out, int32_t* d_ranks, void* d_workspace,
                      void* stream);

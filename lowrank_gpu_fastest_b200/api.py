@@ -100,24 +100,27 @@ def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", retu
 
 
 def _denoise_host(t, patch, stride, batch, form, return_ranks, as_numpy):
+    """Host -> host through ``lrd_denoise_host``: the volume moves in x-slabs
+    on the plan's copy streams while earlier slabs compute; the result lands in
+    pinned host memory (as step8_tuned.py:144-146 copies into pinned)."""
     if t.dim() != 4:
         raise ValueError(f"vol must be 4D (x, y, z, t), got shape {tuple(t.shape)}")
     device = torch.cuda.current_device()
     plan = _plan(t.shape, patch, stride, form, batch, device)
     stream = torch.cuda.current_stream(device)
     ws = _workspace(plan, device, stream.cuda_stream)
-    d_in = torch.empty(t.shape, dtype=torch.float32, device=f"cuda:{device}")
+    dev = f"cuda:{device}"
+    d_in = torch.empty(t.shape, dtype=torch.float32, device=dev)
     d_out = torch.empty_like(d_in)
-    d_in.copy_(t, non_blocking=True)
-    ranks = torch.empty(plan.n_patches, dtype=torch.int32, device=d_in.device) if return_ranks else None
-    plan.denoise(d_in.data_ptr(), d_out.data_ptr(), ranks.data_ptr() if ranks is not None else None,
-                 ws.data_ptr(), stream.cuda_stream)
+    d_ranks = torch.empty(plan.n_patches, dtype=torch.int32, device=dev)
     host = torch.empty(t.shape, dtype=torch.float32, pin_memory=True)
-    host.copy_(d_out)  # synchronous w.r.t. the host: the result is ready on return
+    h_ranks = torch.empty(plan.n_patches, dtype=torch.int32, pin_memory=True) if return_ranks else None
+    src = t.contiguous()
+    plan.denoise_host(src.data_ptr(), host.data_ptr(), h_ranks.data_ptr() if h_ranks is not None else None,
+                      d_in.data_ptr(), d_out.data_ptr(), d_ranks.data_ptr(), ws.data_ptr(), stream.cuda_stream)
     res = host.numpy() if as_numpy else host
     if return_ranks:
-        r = ranks.cpu()
-        return res, (r.numpy() if as_numpy else r)
+        return res, (h_ranks.numpy() if as_numpy else h_ranks)
     return res
 
 

@@ -514,8 +514,10 @@ __host__ __device__ inline size_t eigh_refine_smem_bytes(int n, int pz) {
   return sizeof(double) * eigh_smem_elems(n) + sizeof(float) * (size_t)pz * n;
 }
 
-// Float64 pass over the queued near-tie patches: persistent grid, one patch
-// per block at a time. The block forms G = Xc^T Xc in float64 (products of the
+// Float64 pass over the queued near-tie patches not yet refined:
+// refine_count[0] = entries queued, refine_count[1] = entries already refined
+// (advanced by refine_advance_kernel after this kernel). Persistent grid, one
+// patch per block at a time. The block forms G = Xc^T Xc in float64 (products of the
 // float32 centred values are exact in float64, the sum is float64), then warp
 // 0 runs the float64 eigensolver and overwrites the patch's rank, weight,
 // eigenvectors (and eigenvalues if requested).
@@ -527,11 +529,12 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
   const int lda = eigh_lda(n);
   double* A = sm_ref;
   float* run = reinterpret_cast<float*>(sm_ref + eigh_smem_elems(n));
-  const int count = *refine_count;
+  const int count = refine_count[0];
+  const int first = refine_count[1];
   const int tid = threadIdx.x;
   const int nth = blockDim.x;
   const int nent = n * (n + 1) / 2;
-  for (int w = blockIdx.x; w < count; w += gridDim.x) {
+  for (int w = first + blockIdx.x; w < count; w += gridDim.x) {
     const long long pid = refine_ids[w];
     int ci, cj, ck;
     patch_axes(g, pid, ci, cj, ck);
@@ -581,5 +584,8 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
     __syncthreads();
   }
 }
+
+// Marks every queued near-tie patch as refined (one thread).
+__global__ void refine_advance_kernel(int* refine_count) { refine_count[1] = refine_count[0]; }
 
 }  // namespace lrd

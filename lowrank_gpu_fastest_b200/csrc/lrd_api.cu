@@ -82,6 +82,10 @@ struct lrd_plan {
   // device tables (one allocation)
   void* d_tables;
   lrd::AxisTables tab;
+  // host copies of the x-axis tables (host-buffer pipeline) and its streams/events
+  std::vector<int32_t> h_corner_x, h_brick_x;
+  cudaStream_t io_in = nullptr, io_out = nullptr;
+  std::vector<cudaEvent_t> io_events;  // 2 per slab + 1
   // measurement hook: a ring of per-call phase events
   bool profiling = false;
   int prof_calls = 0;
@@ -90,6 +94,7 @@ struct lrd_plan {
 
 namespace {
 constexpr int kProfRing = 256;
+constexpr int kIoSlabs = 8;  // x-slabs of the host-buffer pipeline
 }
 
 namespace {
@@ -248,13 +253,18 @@ int launch_check(const char* what) {
   return LRD_OK;
 }
 
-int run_center(const lrd_plan* P, const float* d_vol, char* ws, cudaStream_t st) {
+// Centre voxel rows [v0, v0 + nv).
+int run_center(const lrd_plan* P, const float* d_vol, char* ws, cudaStream_t st, long long v0 = 0,
+               long long nv = -1) {
+  if (nv < 0) nv = P->nvox - v0;
+  if (nv <= 0) return LRD_OK;
   float* mean = reinterpret_cast<float*>(ws + P->off_mean);
   float* xc = reinterpret_cast<float*>(ws + P->off_xc);
+  const int T = P->g.nt;
   const long long per_block = 32LL * P->center_warps;
-  const long long blocks = (P->nvox + per_block - 1) / per_block;
+  const long long blocks = (nv + per_block - 1) / per_block;
   lrd::center_kernel<<<(unsigned)blocks, 32 * P->center_warps, P->smem_center, st>>>(
-      d_vol, xc, mean, P->nvox, P->g.nt);
+      d_vol + v0 * T, xc + v0 * T, mean + v0, nv, T);
   return launch_check("center_kernel launch");
 }
 
@@ -290,18 +300,23 @@ int encode_plane_map(const lrd_plan* P, const float* xc, CUtensorMap* map) {
   return LRD_OK;
 }
 
-int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
+// Gram matrices of the patch columns [col_lo, col_hi) (x-major column index
+// ci * ncy + cj; -1 = all), i.e. of patches [col_lo * ncz, col_hi * ncz).
+int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long long col_lo = 0,
+             long long col_hi = -1) {
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
+  const long long ncol = (long long)P->g.ncx * P->g.ncy;
+  if (col_hi < 0) col_hi = ncol;
+  if (col_hi <= col_lo) return LRD_OK;
+  const long long TT = (long long)P->g.nt * P->g.nt;
   if (P->use_gramz || P->use_gramtc) {
     CUtensorMap map;
     int rc = encode_plane_map(P, xc, &map);
     if (rc) return rc;
     int* status = reinterpret_cast<int*>(ws + P->off_status);
-    const long long ncol = (long long)P->g.ncx * P->g.ncy;
     const long long cols = P->prob.batch > 0 ? std::max<long long>(1, P->prob.batch / P->g.ncz) : ncol;
-    const long long TT = (long long)P->g.nt * P->g.nt;
-    for (long long c0 = 0; c0 < ncol; c0 += cols) {
-      const long long nc = std::min(cols, ncol - c0);
+    for (long long c0 = col_lo; c0 < col_hi; c0 += cols) {
+      const long long nc = std::min(cols, col_hi - c0);
       if (P->use_gramtc) {
         lrd::gram_tc_kernel<<<(unsigned)nc, 128, P->smem_gramtc, st>>>(map, d_gram + c0 * P->g.ncz * TT, P->g,
                                                                       P->tab, c0, P->gramz_ring, status);
@@ -315,11 +330,10 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
     }
     return LRD_OK;
   }
-  const long long npatch = P->g.npatch;
-  const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
-  const long long TT = (long long)P->g.nt * P->g.nt;
-  for (long long p0 = 0; p0 < npatch; p0 += batch) {
-    const long long nb = std::min(batch, npatch - p0);
+  const long long p_lo = col_lo * P->g.ncz, p_hi = col_hi * P->g.ncz;
+  const long long batch = P->prob.batch > 0 ? P->prob.batch : (p_hi - p_lo);
+  for (long long p0 = p_lo; p0 < p_hi; p0 += batch) {
+    const long long nb = std::min(batch, p_hi - p0);
     lrd::gram_kernel<<<(unsigned)nb, P->gram_threads, P->smem_gram, st>>>(xc, d_gram + p0 * TT, P->g,
                                                                          P->tab, p0);
     int rc = launch_check("gram_kernel launch");
@@ -328,20 +342,22 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st) {
   return LRD_OK;
 }
 
-// Float32 eigensolver over all patches, then the float64 pass over the
-// near-tie patches it queued (the queue lives in the workspace; the centred
-// volume there is the one the Gram was formed from).
+// Float32 eigensolver over patches [p_lo, p_hi) (-1 = all), then the float64
+// pass over the near-tie patches it queued (the queue lives in the workspace:
+// [count, refined, 62 unused, ids...]; the centred volume there is the one
+// the Gram was formed from). ``reset`` clears the queue first.
 int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, float* d_lam, int32_t* d_rank,
-             float* d_wgt, cudaStream_t st) {
+             float* d_wgt, cudaStream_t st, long long p_lo = 0, long long p_hi = -1, bool reset = true) {
   const long long npatch = P->g.npatch;
+  if (p_hi < 0) p_hi = npatch;
   const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
   const int T = P->g.nt;
   const long long TT = (long long)T * T;
   int* rcount = reinterpret_cast<int*>(ws + P->off_refine);
   int* rids = rcount + 64;
-  LRD_CUDA(cudaMemsetAsync(rcount, 0, sizeof(int), st));
-  for (long long p0 = 0; p0 < npatch; p0 += batch) {
-    const long long nb = std::min(batch, npatch - p0);
+  if (reset) LRD_CUDA(cudaMemsetAsync(rcount, 0, 2 * sizeof(int), st));
+  for (long long p0 = p_lo; p0 < p_hi; p0 += batch) {
+    const long long nb = std::min(batch, p_hi - p0);
     const float* gin = d_gram + p0 * TT;
     float* vout = d_vecs + p0 * TT;
     float* lout = d_lam ? d_lam + p0 * T : nullptr;
@@ -363,24 +379,31 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
   lrd::eigh_refine_kernel<<<P->refine_blocks, 128, P->smem_refine, st>>>(xc, d_vecs, d_lam, d_rank, d_wgt, P->g,
                                                                         P->tab, rcount, rids);
-  return launch_check("eigh_refine_kernel launch");
+  int rc = launch_check("eigh_refine_kernel launch");
+  if (rc) return rc;
+  lrd::refine_advance_kernel<<<1, 1, 0, st>>>(rcount);
+  return launch_check("refine_advance_kernel launch");
 }
 
-int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st) {
+// Reconstruction of bricks [b_lo, b_hi) (x-major brick index; -1 = all).
+int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long long b_lo = 0, long long b_hi = -1) {
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
   const float* mean = reinterpret_cast<const float*>(ws + P->off_mean);
   const float* gv = reinterpret_cast<const float*>(ws + P->off_gv);
   const int32_t* rank = reinterpret_cast<const int32_t*>(ws + P->off_rank);
   const float* wgt = reinterpret_cast<const float*>(ws + P->off_wgt);
   const bool acc = P->prob.form != LRD_FORM_PLAIN;
-  const unsigned nbricks = (unsigned)((long long)P->g.nbx * P->g.nby * P->g.nbz);
+  const long long nbricks = (long long)P->g.nbx * P->g.nby * P->g.nbz;
+  if (b_hi < 0) b_hi = nbricks;
+  if (b_hi <= b_lo) return LRD_OK;
   const unsigned threads = (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
   void* fn = recon_kernel_ptr(P->tpt, P->split, acc);
   lrd::Geom g = P->g;
   lrd::AxisTables tab = P->tab;
+  int brick0 = (int)b_lo;
   void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv, (void*)&rank, (void*)&wgt,
-                  (void*)&d_out, (void*)&g, (void*)&tab};
-  cudaError_t e = cudaLaunchKernel(fn, dim3(nbricks), dim3(threads), args, P->smem_recon, st);
+                  (void*)&d_out, (void*)&g, (void*)&tab, (void*)&brick0};
+  cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)(b_hi - b_lo)), dim3(threads), args, P->smem_recon, st);
   if (e != cudaSuccess) return cuda_fail(e, "recon_kernel launch");
   return LRD_OK;
 }
@@ -573,6 +596,27 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
     return fail(LRD_ERR_UNSUPPORTED, "patch plane or T too large for shared memory");
   }
 
+  // host-buffer pipeline: x-axis tables, copy streams, slab events
+  P->h_corner_x = corners[0];
+  P->h_brick_x = brick[0];
+  {
+    cudaError_t e1 = cudaStreamCreateWithFlags(&P->io_in, cudaStreamNonBlocking);
+    cudaError_t e2 = cudaStreamCreateWithFlags(&P->io_out, cudaStreamNonBlocking);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) {
+      lrd_plan_destroy(P);
+      return cuda_fail(e1 != cudaSuccess ? e1 : e2, "cudaStreamCreateWithFlags");
+    }
+    P->io_events.resize(2 * kIoSlabs + 1);
+    for (auto& ev : P->io_events) {
+      cudaError_t e3 = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e3 != cudaSuccess) {
+        ev = nullptr;
+        lrd_plan_destroy(P);
+        return cuda_fail(e3, "cudaEventCreateWithFlags");
+      }
+    }
+  }
+
   // workspace layout
   size_t off = 0;
   P->off_mean = off; off += align256(sizeof(float) * (size_t)nvox);
@@ -621,6 +665,10 @@ int lrd_plan_phase_ms(lrd_plan* P, float* ms, int32_t* n_calls) {
 int lrd_plan_destroy(lrd_plan* P) {
   if (!P) return LRD_OK;
   for (auto& e : P->prof_events) cudaEventDestroy(e);
+  for (auto& e : P->io_events)
+    if (e) cudaEventDestroy(e);
+  if (P->io_in) cudaStreamDestroy(P->io_in);
+  if (P->io_out) cudaStreamDestroy(P->io_out);
   if (P->d_tables) cudaFree(P->d_tables);
   delete P;
   return LRD_OK;
@@ -676,15 +724,68 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
                      float* d_out, int32_t* d_ranks, void* d_ws, void* stream) {
   int rc = check_plan(P);
   if (rc) return rc;
-  if (!h_vol || !h_out || !d_in || !d_out) return fail(LRD_ERR_INVALID, "NULL buffer");
+  if (!h_vol || !h_out || !d_in || !d_out || !d_ws) return fail(LRD_ERR_INVALID, "NULL buffer");
   if (h_ranks && !d_ranks) return fail(LRD_ERR_INVALID, "h_ranks needs d_ranks");
+  if (reinterpret_cast<uintptr_t>(d_ws) % 256) return fail(LRD_ERR_INVALID, "workspace not 256-byte aligned");
+  // Pipeline over x-slabs of patch corners: slab s copies in the x-planes its
+  // patch columns need (copy-in stream), centres them, forms and solves those
+  // columns' patches and refines their near-ties, reconstructs the bricks
+  // whose touching patches are now all final (compute stream = ``stream``),
+  // and copies those bricks' output planes back (copy-out stream). Copies of
+  // one slab overlap the compute of its neighbours.
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const size_t vbytes = sizeof(float) * (size_t)P->nvox * P->g.nt;
-  LRD_CUDA(cudaMemcpyAsync(d_in, h_vol, vbytes, cudaMemcpyHostToDevice, st));
-  if ((rc = lrd_denoise(P, d_in, d_out, d_ranks, d_ws, stream))) return rc;
-  LRD_CUDA(cudaMemcpyAsync(h_out, d_out, vbytes, cudaMemcpyDeviceToHost, st));
-  if (h_ranks)
-    LRD_CUDA(cudaMemcpyAsync(h_ranks, d_ranks, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToHost, st));
+  char* ws = static_cast<char*>(d_ws);
+  const lrd::Geom& g = P->g;
+  const long long plane = (long long)g.ny * g.nz * g.nt;  // floats per x-plane
+  const long long plane_vox = (long long)g.ny * g.nz;
+  float* gv = reinterpret_cast<float*>(ws + P->off_gv);
+  int32_t* rank = reinterpret_cast<int32_t*>(ws + P->off_rank);
+  float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
+  cudaEvent_t start = P->io_events[2 * kIoSlabs];
+  LRD_CUDA(cudaEventRecord(start, st));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_in, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_out, start, 0));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 2 * sizeof(int32_t), st));
+  const int S = std::max(1, std::min(kIoSlabs, g.ncx));
+  int planes_in = 0, ci_done = 0, bx_done = 0;
+  const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
+  for (int s = 0; s < S; ++s) {
+    const int ci_end = (int)((long long)(s + 1) * g.ncx / S);
+    const bool lastslab = s == S - 1;
+    const int x_need = lastslab ? g.nx : std::min(g.nx, P->h_corner_x[ci_end - 1] + g.px);
+    cudaEvent_t ev_in = P->io_events[2 * s], ev_done = P->io_events[2 * s + 1];
+    if (x_need > planes_in)
+      LRD_CUDA(cudaMemcpyAsync(d_in + planes_in * plane, h_vol + planes_in * plane,
+                               sizeof(float) * (size_t)(x_need - planes_in) * plane, cudaMemcpyHostToDevice,
+                               P->io_in));
+    LRD_CUDA(cudaEventRecord(ev_in, P->io_in));
+    LRD_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
+    if ((rc = run_center(P, d_in, ws, st, planes_in * plane_vox, (long long)(x_need - planes_in) * plane_vox)))
+      return rc;
+    planes_in = std::max(planes_in, x_need);
+    if ((rc = run_gram(P, ws, gv, st, ci_done * colz, ci_end * colz))) return rc;
+    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false))) return rc;
+    ci_done = ci_end;
+    int bx_end = bx_done;
+    while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
+    if ((rc = run_recon(P, ws, d_out, st, bx_done * brz, bx_end * brz))) return rc;
+    LRD_CUDA(cudaEventRecord(ev_done, st));
+    if (bx_end > bx_done) {
+      const long long x0 = (long long)bx_done * g.bx, x1 = std::min<long long>((long long)bx_end * g.bx, g.nx);
+      LRD_CUDA(cudaStreamWaitEvent(P->io_out, ev_done, 0));
+      LRD_CUDA(cudaMemcpyAsync(h_out + x0 * plane, d_out + x0 * plane, sizeof(float) * (size_t)(x1 - x0) * plane,
+                               cudaMemcpyDeviceToHost, P->io_out));
+    }
+    bx_done = bx_end;
+  }
+  if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * g.npatch, cudaMemcpyDeviceToDevice, st));
+  if (h_ranks) {
+    LRD_CUDA(cudaEventRecord(P->io_events[2 * S - 1], st));
+    LRD_CUDA(cudaStreamWaitEvent(P->io_out, P->io_events[2 * S - 1], 0));
+    LRD_CUDA(cudaMemcpyAsync(h_ranks, d_ranks, sizeof(int32_t) * g.npatch, cudaMemcpyDeviceToHost, P->io_out));
+  }
+  LRD_CUDA(cudaStreamSynchronize(P->io_out));
   LRD_CUDA(cudaStreamSynchronize(st));
   int32_t status = 0;
   if ((rc = lrd_workspace_status(P, d_ws, &status, stream))) return rc;

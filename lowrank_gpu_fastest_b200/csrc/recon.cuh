@@ -29,8 +29,8 @@
 // contiguous range.
 //
 // Form ACCURATE keeps the temporal mean out of the running sums: it
-// accumulates w * (x - m) V_p V_p^T with a compensated (two-sum) float32
-// accumulator and the weights in float64, then writes m + acc / wsum.
+// accumulates the exact float64 products w * [(x - m) V_p V_p^T] and the
+// weights in float64, then writes m + acc / wsum.
 #pragma once
 
 #include "lrd_common.cuh"
@@ -38,14 +38,6 @@
 namespace lrd {
 
 constexpr int kReconSplit = 4;  // largest number of threads per voxel
-
-__device__ __forceinline__ void two_sum_acc(float& acc, float& comp, float x) {
-  const float s = __fadd_rn(acc, x);
-  const float bp = __fsub_rn(s, acc);
-  const float err = __fadd_rn(__fsub_rn(acc, __fsub_rn(s, bp)), __fsub_rn(x, bp));
-  comp = __fadd_rn(comp, err);
-  acc = s;
-}
 
 __device__ __forceinline__ void cp_async4(float* smem_dst, const float* gmem_src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -66,12 +58,13 @@ __host__ __device__ inline size_t recon_smem_bytes(int T, int max_touch) {
   return sizeof(float) * 2 * (size_t)T * recon_tp(T) + (sizeof(int) + sizeof(float)) * (size_t)max_touch;
 }
 
-// grid: nbx*nby*nbz blocks of bx*by*bz*SPLIT threads (<= 1024).
+// grid: bricks [brick0, brick0 + gridDim.x) of the nbx*nby*nbz (x-major)
+// bricks; bx*by*bz*SPLIT threads per block (<= 1024).
 template <int TPT, int SPLIT, bool ACCURATE>
 __global__ void recon_kernel(const float* __restrict__ xc, const float* __restrict__ mean,
                              const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
                              const float* __restrict__ wgt, float* __restrict__ out, Geom g,
-                             AxisTables tab) {
+                             AxisTables tab, int brick0) {
   extern __shared__ __align__(16) float sm_recon[];
   const int T = g.nt;
   const int TP = recon_tp(T);
@@ -84,7 +77,7 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
   const int vl = tid / SPLIT;
   const int t0 = slice * TPT;
 
-  int brick = blockIdx.x;
+  int brick = brick0 + blockIdx.x;
   const int bzi = brick % g.nbz;
   brick /= g.nbz;
   const int byi = brick % g.nby;
@@ -128,14 +121,17 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
       sm_recon[(size_t)r * TP + c] = 0.f;
     }
 
-  float xr[TPT], acc[TPT], comp[TPT];
+  float xr[TPT], acc[ACCURATE ? 1 : TPT];
+  double acc64[ACCURATE ? TPT : 1];
   float m = 0.f;
 #pragma unroll
   for (int u = 0; u < TPT; ++u) {
     const int t = t0 + u;
     xr[u] = (valid && t < T) ? xc[row * T + t] : 0.f;
-    acc[u] = 0.f;
-    comp[u] = 0.f;
+    if constexpr (ACCURATE)
+      acc64[u] = 0.0;
+    else
+      acc[u] = 0.f;
   }
   if (valid) m = mean[row];
   float wacc = 0.f;
@@ -222,10 +218,11 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
       }
     }
     if (cov) {
-      if (ACCURATE) {
+      if constexpr (ACCURATE) {
+        const double wd = (double)w;
 #pragma unroll
-        for (int u = 0; u < TPT; ++u) two_sum_acc(acc[u], comp[u], __fmul_rn(w, xdp[u]));
-        wacc64 += (double)w;
+        for (int u = 0; u < TPT; ++u) acc64[u] = fma(wd, (double)xdp[u], acc64[u]);
+        wacc64 += wd;
       } else {
 #pragma unroll
         for (int u = 0; u < TPT; ++u) {
@@ -245,7 +242,7 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
     __syncthreads();
   }
   if (!valid) return;
-  if (ACCURATE) {
+  if constexpr (ACCURATE) {
     // a voxel no patch covers (stride > patch side) gets 0, as 0 / max(0, 1e-12)
     // does in the ladder
     const double inv = wacc64 > 0.0 ? 1.0 / wacc64 : 0.0;
@@ -253,7 +250,7 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
       const int t = t0 + u;
-      if (t < T) out[row * T + t] = (float)(mm + ((double)acc[u] + (double)comp[u]) * inv);
+      if (t < T) out[row * T + t] = (float)(mm + acc64[u] * inv);
     }
   } else {
     const float den = fmaxf(wacc, 1e-12f);

@@ -195,3 +195,17 @@ def test_status_word_clear_after_runs(cuda_ok):
         s = torch.cuda.current_stream().cuda_stream
         plan.denoise(vol.data_ptr(), out.data_ptr(), None, ws.data_ptr(), s)
         assert plan.status(ws.data_ptr(), s) == 0
+
+
+@pytest.mark.parametrize("form", ["plain", "tensor"])
+@pytest.mark.parametrize("name", ["headline_ref", "aniso", "lowrank_t96"])
+def test_pipelined_host_call_equals_device_call(cuda_ok, name, form):
+    """lrd_denoise_host (x-slab copy/compute pipeline) gives the device path's
+    output and ranks bit for bit."""
+    g = load_golden(name)
+    vol = golden_input(g)
+    patch, stride = tuple(int(v) for v in g["patch"]), int(g["stride"])
+    host, hr = api.denoise(vol, patch, stride, form=form, return_ranks=True)
+    dev, dr = run_dev(vol, patch, stride, form=form)
+    np.testing.assert_array_equal(host, dev)
+    np.testing.assert_array_equal(hr, dr)
