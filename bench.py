@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="patches in the CPU sample (0 = auto)")
     ap.add_argument("--brick", default=None, help="recon brick bx,by,bz (default: the plan's choice)")
     ap.add_argument("--split", type=int, default=0, help="recon threads per voxel (0 = the plan's choice)")
+    ap.add_argument("--parallel", choices=["shard", "replica"], default="shard",
+                    help="N>1: one (96N)-plane volume cut in N x-slabs with a halo exchange (shard), "
+                         "or one volume per GPU (replica)")
     return ap.parse_args()
 
 
@@ -410,13 +413,126 @@ def run_ours(args, wl):
                            achieved_tflops_gram_recon=total_flops / ((ph["gram"] + ph["recon"]) * 1e-3) / 1e12),
             cpu_baseline=cpu,
             clocks=clocks,
-            gpu_launches=4 * args.steps if (plan.problem.batch == 0) else None,
+            gpu_launches=6 * args.steps,
+            gpu_launches_note="per step: center, gram (column TMA or tensor), eigh, eigh_refine, "
+                              "refine_advance, recon (plus two status memsets)",
             wall_s_timed_region=wall,
         )
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_sharded(args, wl):
+    """N GPUs, one volume: the workload's volume repeated N times along x
+    ((X*N, Y, Z, T)), its x-corners cut in N slabs (one per rank), one NCCL
+    halo exchange between neighbours per step. Per-GPU work is about the
+    single-GPU workload's (weak scaling)."""
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+    from lowrank_gpu_fastest_b200.problem import n_patches
+    from lowrank_gpu_fastest_b200.shard import CudaSlab, run_slab, slab_partition
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    X, Y, Z, T = wl["shape"]
+    gshape = (X * world, Y, Z, T)
+    patch, stride = wl["patch"], wl["stride"]
+    parts = slab_partition(gshape, patch, stride, world)
+    me = parts[rank]
+    base, _ = make_phantom_lowrank(wl["shape"], seed=0)
+    planes = np.ascontiguousarray(np.take(base, np.arange(me["x0"], me["x1"]) % X, axis=0))
+    slab = CudaSlab(gshape, rank, world, patch, stride, args.form, device=local)
+    h_in = torch.from_numpy(planes).pin_memory()
+    own = slab.own[1] - slab.own[0]
+    h_out = torch.empty((own, Y, Z, T), dtype=torch.float32, pin_memory=True)
+    slab.load(h_in)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    P_total = n_patches(gshape, patch, stride)
+    # this rank's kernels per step: centre, Gram, eigensolve, refine, refine cursor, and one
+    # reconstruction per non-empty part (halo out, interior, halo in)
+    launches = 5 + int(slab.halo_out.numel() > 0) + int(slab.own[1] - slab.own[0] > slab.plan.hin) + \
+        int(slab.plan.hin > 0)
+
+    def step():
+        run_slab(slab, rank, world)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    dist.barrier()
+    torch.cuda.synchronize()
+    for s, e in evs:
+        flush.zero_()
+        s.record(stream)
+        step()
+        e.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    t = torch.tensor([sum(s.elapsed_time(e) for s, e in evs)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t.item()) / args.steps
+    value = P_total / (ms_per_step * 1e-3)
+
+    # e2e: the slab's planes from pinned host memory, the step, the owned planes back
+    def e2e_step():
+        slab.vol.copy_(h_in, non_blocking=True)
+        run_slab(slab, rank, world)
+        h_out.copy_(slab.owned(), non_blocking=True)
+        torch.cuda.synchronize()
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    dist.barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    t = torch.tensor([statistics.mean(e2e_ms)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms_step = float(t.item())
+    halo_bytes = slab.halo_out.numel() * 8
+    if rank == 0:
+        line = dict(
+            metric="patches_per_s", value=value, unit="patches/s", n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=ms_per_step, ms_per_volume=ms_per_step,
+            higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+            config=dict(workload=f"{wl['desc']} repeated {world}x along x, cut in {world} x-slabs",
+                        shape=list(gshape), patch=list(patch), stride=stride, form=args.form,
+                        phantom="rank-4 [0,1] + N(0,0.05^2) seed 0, tiled along x",
+                        l2="flushed by a 256 MiB write between timed steps (outside the events)",
+                        parallelism=f"x-slab shard x{world}, NCCL send/recv halo "
+                                    f"({halo_bytes / 1e6:.1f} MB per boundary)",
+                        patches=P_total),
+            e2e=dict(value=P_total / (e2e_ms_step * 1e-3), unit="patches/s", ms_per_step=e2e_ms_step,
+                     h2d_bytes_per_step=int(h_in.numel() * 4), d2h_bytes_per_step=int(h_out.numel() * 4),
+                     path="per rank: H2D of its slab planes, slab step with halo exchange, D2H of owned "
+                          "planes (rank 0's bytes; max time over ranks)"),
+            clocks=clocks,
+            gpu_launches=launches * args.steps,
+            gpu_launches_note="rank 0's own kernels (NCCL's send/recv kernels not counted)",
+        )
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
 
 
 def run_batched(args):
@@ -519,6 +635,8 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)
+    elif dist_env()[1] > 1 and args.parallel == "shard":
+        run_sharded(args, wl)
     else:
         run_ours(args, wl)
 

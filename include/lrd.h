@@ -196,6 +196,49 @@ int lrd_batch_workspace_size(const lrd_batch_plan* plan, size_t* bytes);
 int lrd_batch_denoise(lrd_batch_plan* plan, const float* const* d_vols, float* const* d_outs,
                       int32_t* const* d_ranks, void* d_workspace, void* stream, int32_t use_graph);
 
+/* Slab sharding: one volume over several GPUs (one process per GPU), cut by
+ * x-corner. Replaces, for a volume too large or too slow for one GPU, the
+ * ladder's single ``denoise`` call (step0_numpy_loop.py:28-39; corners from
+ * common.py:40-43).
+ *
+ * The x-corner list is cut into n_slabs contiguous runs of about equal
+ * length. Slab r reads global x-planes [x0, x1): from its first corner to the
+ * last plane its patches touch (the last slab to the volume's end), and owns
+ * the output planes [x0, x0 of slab r+1). Its top planes [x0 of slab r+1, x1)
+ * are also touched by slab r+1's patches: slab r hands its unnormalised sums
+ * (sum of w * xd per frame, then sum of w, float64) for those planes to slab
+ * r+1, which continues them with its own patches. A voxel's patches are
+ * therefore added in the single-GPU (x-major) order and every slab's owned
+ * planes equal the single-GPU output bit for bit. No voxel may be touched by
+ * three slabs (LRD_ERR_UNSUPPORTED otherwise: use fewer slabs).
+ *
+ * lrd_slab_partition fills bounds[4*r .. 4*r+3] = {first corner index, end
+ * corner index, x0, x1} for each slab r. lrd_slab_plan_create makes the plan
+ * of slab ``slab`` (its local volume is planes [x0, x1) of the global one;
+ * workspace and buffers sized by the plan as for lrd_plan_create).
+ * lrd_slab_info gives info[0..7] = {x0, local planes nx, halo-in planes hin,
+ * owned planes own_hi, first corner, end corner, slab, n_slabs}; the halo a
+ * slab receives is hin x ny x nz x (nt + 1) doubles, the one it sends
+ * (nx - own_hi) x ny x nz x (nt + 1).
+ *
+ * lrd_slab_prepare runs centring, Gram, eigensolve and MP rank for the slab's
+ * patches (ranks -> d_ranks, nullable). lrd_slab_recon then reconstructs one
+ * part of the local planes: LRD_SLAB_HALO_OUT (planes [own_hi, nx), sums ->
+ * d_halo_out), LRD_SLAB_INTERIOR (planes [hin, own_hi) -> d_out) or
+ * LRD_SLAB_HALO_IN (planes [0, hin), continuing from d_halo_in -> d_out).
+ * d_out has the local volume's shape; only the owned planes are written. The
+ * halo pointers are ignored by the parts that do not use them. */
+#define LRD_SLAB_HALO_OUT 0
+#define LRD_SLAB_INTERIOR 1
+#define LRD_SLAB_HALO_IN 2
+int lrd_slab_partition(const lrd_problem* problem, int32_t n_slabs, int32_t* bounds);
+int lrd_slab_plan_create(const lrd_problem* problem, int32_t n_slabs, int32_t slab, lrd_plan** plan);
+int lrd_slab_info(const lrd_plan* plan, int32_t* info);
+int lrd_slab_prepare(const lrd_plan* plan, const float* d_vol, int32_t* d_ranks, void* d_workspace,
+                     void* stream);
+int lrd_slab_recon(const lrd_plan* plan, float* d_out, void* d_workspace, int32_t part,
+                   const double* d_halo_in, double* d_halo_out, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* lrd_last_error_string(void);
 int lrd_version(void);

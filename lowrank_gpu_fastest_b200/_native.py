@@ -48,7 +48,15 @@ SIGNATURES = {
     "lrd_batch_denoise": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int32]),
     "lrd_workspace_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.c_void_p]),
+    "lrd_slab_partition": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _c_i32p]),
+    "lrd_slab_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+    "lrd_slab_info": (ctypes.c_int, [ctypes.c_void_p, _c_i32p]),
+    "lrd_slab_prepare": (ctypes.c_int, [ctypes.c_void_p] * 5),
+    "lrd_slab_recon": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
+SLAB_HALO_OUT, SLAB_INTERIOR, SLAB_HALO_IN = 0, 1, 2
 PHASES = ("center", "gram", "eigh_mp", "recon")
 
 
@@ -96,24 +104,44 @@ def check(rc: int):
         raise LrdError(rc, msg)
 
 
+def make_problem(shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0):
+    if form not in FORMS:
+        raise ValueError(f"form must be one of {sorted(FORMS)}, got {form!r}")
+    nx, ny, nz, nt = (int(s) for s in shape)
+    px, py, pz = (int(p) for p in patch)
+    bx, by, bz = (int(b) for b in (brick or (0, 0, 0)))
+    return LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0),
+                      bx, by, bz, int(split or 0))
+
+
+def slab_partition(shape, patch, stride, n_slabs):
+    """Per slab ``(first corner, end corner, x0, x1)`` (``lrd_slab_partition``;
+    host-only, no device needed)."""
+    pr = make_problem(shape, patch, stride)
+    b = (ctypes.c_int32 * (4 * int(n_slabs)))()
+    check(load().lrd_slab_partition(ctypes.byref(pr), int(n_slabs), b))
+    v = list(b)
+    return [tuple(v[4 * r:4 * r + 4]) for r in range(int(n_slabs))]
+
+
 class Plan:
     """Owns an ``lrd_plan*`` for one problem on the current CUDA device."""
 
-    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0):
+    def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0,
+                 _slab=None):
         lib = load()
-        if form not in FORMS:
-            raise ValueError(f"form must be one of {sorted(FORMS)}, got {form!r}")
+        self.problem = make_problem(shape, patch, stride, form, batch, brick, split)
         nx, ny, nz, nt = (int(s) for s in shape)
-        px, py, pz = (int(p) for p in patch)
-        bx, by, bz = (int(b) for b in (brick or (0, 0, 0)))
-        self.problem = LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0),
-                                  bx, by, bz, int(split or 0))
         self.shape = (nx, ny, nz, nt)
-        self.patch = (px, py, pz)
+        self.patch = tuple(int(p) for p in patch)
         self.stride = int(stride)
         self.form = form
         h = ctypes.c_void_p()
-        check(lib.lrd_plan_create(ctypes.byref(self.problem), ctypes.byref(h)))
+        if _slab is None:
+            check(lib.lrd_plan_create(ctypes.byref(self.problem), ctypes.byref(h)))
+        else:
+            check(lib.lrd_slab_plan_create(ctypes.byref(self.problem), int(_slab[1]), int(_slab[0]),
+                                           ctypes.byref(h)))
         self.handle = h
         n = ctypes.c_int64()
         check(lib.lrd_plan_num_patches(h, ctypes.byref(n)))
@@ -159,6 +187,25 @@ class Plan:
 
     def stage_eigh(self, d_gram, d_lam, d_vecs, d_ranks, d_ws, stream):
         check(load().lrd_stage_eigh(self.handle, d_gram, d_lam, d_vecs, d_ranks, d_ws, stream))
+
+
+class SlabPlan(Plan):
+    """Plan of slab ``slab`` of ``n_slabs`` of a volume of ``shape`` (global)."""
+
+    def __init__(self, shape, slab, n_slabs, patch=(11, 11, 11), stride=3, form="plain", brick=None, split=0):
+        super().__init__(shape, patch, stride, form, 0, brick, split, _slab=(slab, n_slabs))
+        info = (ctypes.c_int32 * 8)()
+        check(load().lrd_slab_info(self.handle, info))
+        (self.x0, self.nx, self.hin, self.own_hi, self.ci_lo, self.ci_hi, self.slab,
+         self.n_slabs) = (int(v) for v in info)
+        self.global_shape = self.shape
+        self.shape = (self.nx,) + self.global_shape[1:]
+
+    def prepare(self, d_vol, d_ranks, d_ws, stream):
+        check(load().lrd_slab_prepare(self.handle, d_vol, d_ranks, d_ws, stream))
+
+    def recon(self, part, d_out, d_ws, d_halo_in, d_halo_out, stream):
+        check(load().lrd_slab_recon(self.handle, d_out, d_ws, int(part), d_halo_in, d_halo_out, stream))
 
 
 class BatchPlan:

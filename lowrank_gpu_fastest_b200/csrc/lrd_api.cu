@@ -90,6 +90,11 @@ struct lrd_plan {
   bool profiling = false;
   int prof_calls = 0;
   std::vector<cudaEvent_t> prof_events;  // kProfRing * (LRD_NUM_PHASES + 1)
+  // slab of a sharded volume: local plane 0 is global plane slab_x0; planes
+  // [0, slab_hin) continue the lower slab's sums, planes [slab_own_hi, nx) are
+  // handed to the upper slab
+  bool is_slab = false;
+  int slab_x0 = 0, slab_hin = 0, slab_own_hi = 0, slab_ci_lo = 0, slab_ci_hi = 0, slab = 0, n_slabs = 1;
 };
 
 namespace {
@@ -386,7 +391,10 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
 }
 
 // Reconstruction of bricks [b_lo, b_hi) (x-major brick index; -1 = all).
-int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long long b_lo = 0, long long b_hi = -1) {
+// ``io`` restricts the voxels to an x-range and routes slab halos (slab
+// sharding); nullptr = every voxel, normalised into ``d_out``.
+int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long long b_lo = 0, long long b_hi = -1,
+              const lrd::SlabIO* io = nullptr) {
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
   const float* mean = reinterpret_cast<const float*>(ws + P->off_mean);
   const float* gv = reinterpret_cast<const float*>(ws + P->off_gv);
@@ -401,8 +409,10 @@ int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long l
   lrd::Geom g = P->g;
   lrd::AxisTables tab = P->tab;
   int brick0 = (int)b_lo;
+  lrd::SlabIO sio{0, g.nx, 0, nullptr, g.nx, nullptr};
+  if (io) sio = *io;
   void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv, (void*)&rank, (void*)&wgt,
-                  (void*)&d_out, (void*)&g, (void*)&tab, (void*)&brick0};
+                  (void*)&d_out, (void*)&g, (void*)&tab, (void*)&brick0, (void*)&sio};
   cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)(b_hi - b_lo)), dim3(threads), args, P->smem_recon, st);
   if (e != cudaSuccess) return cuda_fail(e, "recon_kernel launch");
   return LRD_OK;
@@ -418,15 +428,10 @@ int check_plan(const lrd_plan* P) {
   return LRD_OK;
 }
 
-}  // namespace
-
-extern "C" {
-
-int lrd_version(void) { return LRD_VERSION; }
-
-const char* lrd_last_error_string(void) { return g_last_error.c_str(); }
-
-int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
+// Plan for ``pr``; ``x_corners`` (nullable) replaces the x-axis corner list
+// (a slab of a larger volume), which must be sorted, start >= 0 and end
+// with a patch inside the volume.
+int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lrd_plan** out) {
   g_last_error.clear();
   if (!pr || !out) return fail(LRD_ERR_INVALID, "problem or plan pointer is NULL");
   *out = nullptr;
@@ -457,7 +462,7 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
 
   std::vector<int32_t> corners[3], cover[3], brick[3];
   for (int a = 0; a < 3; ++a) {
-    corners[a] = axis_corners(dims[a], pat[a], pr->stride);
+    corners[a] = (a == 0 && x_corners) ? *x_corners : axis_corners(dims[a], pat[a], pr->stride);
     cover[a].resize(2 * (size_t)dims[a]);
     for (int x = 0; x < dims[a]; ++x) {
       int lo = -1, hi = -2;
@@ -631,6 +636,42 @@ int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) {
   return LRD_OK;
 }
 
+// Cut of the x-corner list into n contiguous slabs: per slab {first corner,
+// end corner, first plane read, end plane read}. Slab r owns output planes
+// [x0(r), x0(r + 1)); the planes [x0(r + 1), x1(r)) are touched by both.
+int slab_partition(const lrd_problem* pr, int n, std::vector<int32_t>& b) {
+  if (!pr) return fail(LRD_ERR_INVALID, "problem is NULL");
+  if (pr->nx < 1 || pr->px < 1 || pr->px > pr->nx || pr->stride < 1)
+    return fail(LRD_ERR_INVALID, "bad x axis (nx %d, px %d, stride %d)", pr->nx, pr->px, pr->stride);
+  const std::vector<int32_t> cx = axis_corners(pr->nx, pr->px, pr->stride);
+  const int nc = (int)cx.size();
+  if (n < 1 || n > nc) return fail(LRD_ERR_INVALID, "n_slabs=%d must be in [1, %d] (x-corners)", n, nc);
+  b.assign(4 * (size_t)n, 0);
+  for (int r = 0; r < n; ++r) {
+    b[4 * r] = (int32_t)((long long)r * nc / n);
+    b[4 * r + 1] = (int32_t)((long long)(r + 1) * nc / n);
+    b[4 * r + 2] = r == 0 ? 0 : cx[b[4 * r]];
+  }
+  for (int r = 0; r < n; ++r)
+    b[4 * r + 3] = r == n - 1 ? pr->nx : std::max(cx[b[4 * r + 1] - 1] + pr->px, b[4 * (r + 1) + 2]);
+  for (int r = 0; r + 2 < n; ++r)
+    if (b[4 * r + 3] > b[4 * (r + 2) + 2])
+      return fail(LRD_ERR_UNSUPPORTED,
+                  "%d slabs: planes [%d, %d) would be touched by three slabs; use fewer slabs", n,
+                  b[4 * (r + 2) + 2], b[4 * r + 3]);
+  return LRD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lrd_version(void) { return LRD_VERSION; }
+
+const char* lrd_last_error_string(void) { return g_last_error.c_str(); }
+
+int lrd_plan_create(const lrd_problem* pr, lrd_plan** out) { return create_plan(pr, nullptr, out); }
+
 int lrd_plan_set_profiling(lrd_plan* P, int enable) {
   if (!P) return fail(LRD_ERR_INVALID, "plan is NULL");
   if (enable && P->prof_events.empty()) {
@@ -791,6 +832,103 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   if ((rc = lrd_workspace_status(P, d_ws, &status, stream))) return rc;
   if (status) return fail(LRD_ERR_TIMEOUT, "a device wait gave up (status 0x%x): the result is invalid", status);
   return LRD_OK;
+}
+
+int lrd_slab_partition(const lrd_problem* pr, int32_t n, int32_t* bounds) {
+  g_last_error.clear();
+  if (!bounds) return fail(LRD_ERR_INVALID, "bounds is NULL");
+  std::vector<int32_t> b;
+  int rc = slab_partition(pr, n, b);
+  if (rc) return rc;
+  memcpy(bounds, b.data(), b.size() * sizeof(int32_t));
+  return LRD_OK;
+}
+
+int lrd_slab_plan_create(const lrd_problem* pr, int32_t n, int32_t slab, lrd_plan** out) {
+  g_last_error.clear();
+  if (!out) return fail(LRD_ERR_INVALID, "plan pointer is NULL");
+  *out = nullptr;
+  std::vector<int32_t> b;
+  int rc = slab_partition(pr, n, b);
+  if (rc) return rc;
+  if (slab < 0 || slab >= n) return fail(LRD_ERR_INVALID, "slab %d not in [0, %d)", slab, n);
+  const int ci_lo = b[4 * slab], ci_hi = b[4 * slab + 1], x0 = b[4 * slab + 2], x1 = b[4 * slab + 3];
+  const std::vector<int32_t> cx = axis_corners(pr->nx, pr->px, pr->stride);
+  std::vector<int32_t> local(cx.begin() + ci_lo, cx.begin() + ci_hi);
+  for (auto& c : local) c -= x0;
+  lrd_problem lp = *pr;
+  lp.nx = x1 - x0;
+  lrd_plan* P = nullptr;
+  if ((rc = create_plan(&lp, &local, &P))) return rc;
+  P->is_slab = true;
+  P->slab = slab;
+  P->n_slabs = n;
+  P->slab_x0 = x0;
+  P->slab_ci_lo = ci_lo;
+  P->slab_ci_hi = ci_hi;
+  P->slab_hin = slab == 0 ? 0 : b[4 * (slab - 1) + 3] - x0;
+  P->slab_own_hi = slab == n - 1 ? lp.nx : b[4 * (slab + 1) + 2] - x0;
+  *out = P;
+  return LRD_OK;
+}
+
+int lrd_slab_info(const lrd_plan* P, int32_t* info) {
+  if (!P || !info) return fail(LRD_ERR_INVALID, "NULL argument");
+  if (!P->is_slab) return fail(LRD_ERR_INVALID, "not a slab plan");
+  const int32_t v[8] = {P->slab_x0, P->g.nx, P->slab_hin, P->slab_own_hi,
+                        P->slab_ci_lo, P->slab_ci_hi, P->slab, P->n_slabs};
+  memcpy(info, v, sizeof(v));
+  return LRD_OK;
+}
+
+int lrd_slab_prepare(const lrd_plan* P, const float* d_vol, int32_t* d_ranks, void* d_ws, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!P->is_slab) return fail(LRD_ERR_INVALID, "not a slab plan");
+  if (!d_vol || !d_ws) return fail(LRD_ERR_INVALID, "NULL device buffer");
+  if (reinterpret_cast<uintptr_t>(d_ws) % 256) return fail(LRD_ERR_INVALID, "workspace not 256-byte aligned");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(d_ws);
+  float* gv = reinterpret_cast<float*>(ws + P->off_gv);
+  int32_t* rank = reinterpret_cast<int32_t*>(ws + P->off_rank);
+  float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
+  if ((rc = run_center(P, d_vol, ws, st))) return rc;
+  if ((rc = run_gram(P, ws, gv, st))) return rc;
+  if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st))) return rc;
+  if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToDevice, st));
+  return LRD_OK;
+}
+
+int lrd_slab_recon(const lrd_plan* P, float* d_out, void* d_ws, int32_t part, const double* d_halo_in,
+                   double* d_halo_out, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!P->is_slab) return fail(LRD_ERR_INVALID, "not a slab plan");
+  if (!d_ws) return fail(LRD_ERR_INVALID, "NULL workspace");
+  lrd::SlabIO io{0, 0, P->slab_hin, nullptr, P->slab_own_hi, nullptr};
+  if (part == LRD_SLAB_HALO_OUT) {
+    io.x_lo = P->slab_own_hi;
+    io.x_hi = P->g.nx;
+    io.halo_out = d_halo_out;
+    if (io.x_lo < io.x_hi && !d_halo_out) return fail(LRD_ERR_INVALID, "d_halo_out is NULL");
+  } else if (part == LRD_SLAB_INTERIOR) {
+    io.x_lo = P->slab_hin;
+    io.x_hi = P->slab_own_hi;
+  } else if (part == LRD_SLAB_HALO_IN) {
+    io.x_lo = 0;
+    io.x_hi = P->slab_hin;
+    io.halo_in = d_halo_in;
+    if (io.x_lo < io.x_hi && !d_halo_in) return fail(LRD_ERR_INVALID, "d_halo_in is NULL");
+  } else {
+    return fail(LRD_ERR_INVALID, "unknown slab part %d", part);
+  }
+  if (io.x_lo >= io.x_hi) return LRD_OK;
+  if (part != LRD_SLAB_HALO_OUT && !d_out) return fail(LRD_ERR_INVALID, "d_out is NULL");
+  const long long brz = (long long)P->g.nby * P->g.nbz;
+  const long long b_lo = (long long)(io.x_lo / P->g.bx) * brz;
+  const long long b_hi = (long long)((io.x_hi + P->g.bx - 1) / P->g.bx) * brz;
+  return run_recon(P, static_cast<char*>(d_ws), d_out, static_cast<cudaStream_t>(stream), b_lo, b_hi, &io);
 }
 
 int lrd_workspace_status(const lrd_plan* P, const void* d_ws, int32_t* status, void* stream) {

@@ -58,13 +58,26 @@ __host__ __device__ inline size_t recon_smem_bytes(int T, int max_touch) {
   return sizeof(float) * 2 * (size_t)T * recon_tp(T) + (sizeof(int) + sizeof(float)) * (size_t)max_touch;
 }
 
+// Slab sharding of one volume over GPUs (x-slabs of patch corners): which
+// voxels a launch computes, and the partial sums handed between neighbours.
+// A voxel's patches are accumulated in x-major order, so a lower slab's
+// partial (sum and weight of its patches, in order) followed by this slab's
+// patches is exactly the single-GPU sequence.
+struct SlabIO {
+  int x_lo, x_hi;         // voxels with x in [x_lo, x_hi) are computed
+  int hin;                // planes [0, hin) start from halo_in (nullable)
+  const double* halo_in;  // (hin, ny, nz, T + 1): T sums then the weight sum
+  int own_hi;             // planes >= own_hi go to halo_out unnormalised
+  double* halo_out;       // (nx - own_hi, ny, nz, T + 1)
+};
+
 // grid: bricks [brick0, brick0 + gridDim.x) of the nbx*nby*nbz (x-major)
 // bricks; bx*by*bz*SPLIT threads per block (<= 1024).
 template <int TPT, int SPLIT, bool ACCURATE>
 __global__ void recon_kernel(const float* __restrict__ xc, const float* __restrict__ mean,
                              const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
                              const float* __restrict__ wgt, float* __restrict__ out, Geom g,
-                             AxisTables tab, int brick0) {
+                             AxisTables tab, int brick0, SlabIO io) {
   extern __shared__ __align__(16) float sm_recon[];
   const int T = g.nt;
   const int TP = recon_tp(T);
@@ -86,7 +99,7 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
   const int bvox = g.bx * g.by * g.bz;
   const int lz = vl % g.bz, ly = (vl / g.bz) % g.by, lx = vl / (g.by * g.bz);
   const int x = bxi * g.bx + lx, y = byi * g.by + ly, z = bzi * g.bz + lz;
-  const bool valid = vl < bvox && x < g.nx && y < g.ny && z < g.nz;
+  const bool valid = vl < bvox && x < g.nx && y < g.ny && z < g.nz && x >= io.x_lo && x < io.x_hi;
 
   int cxlo = 1, cxhi = 0, cylo = 1, cyhi = 0, czlo = 1, czhi = 0;
   long long row = 0;
@@ -136,6 +149,21 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
   if (valid) m = mean[row];
   float wacc = 0.f;
   double wacc64 = 0.0;
+  if (valid && x < io.hin && io.halo_in != nullptr) {  // continue a lower slab's sums
+    const double* hp = io.halo_in + row * (T + 1);
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) {
+      const int t = t0 + u;
+      if (t < T) {
+        if constexpr (ACCURATE)
+          acc64[u] = hp[t];
+        else
+          acc[u] = (float)hp[t];
+      }
+    }
+    wacc64 = hp[T];
+    wacc = (float)hp[T];
+  }
   __syncthreads();
 
   const bool vec16 = (T & 3) == 0;
@@ -242,6 +270,21 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
     __syncthreads();
   }
   if (!valid) return;
+  if (x >= io.own_hi) {  // the next slab's halo: unnormalised sums in patch order
+    double* hp = io.halo_out + (row - (long long)io.own_hi * g.ny * g.nz) * (T + 1);
+#pragma unroll
+    for (int u = 0; u < TPT; ++u) {
+      const int t = t0 + u;
+      if (t < T) {
+        if constexpr (ACCURATE)
+          hp[t] = acc64[u];
+        else
+          hp[t] = (double)acc[u];
+      }
+    }
+    if (slice == 0) hp[T] = ACCURATE ? wacc64 : (double)wacc;
+    return;
+  }
   if constexpr (ACCURATE) {
     // a voxel no patch covers (stride > patch side) gets 0, as 0 / max(0, 1e-12)
     // does in the ladder
