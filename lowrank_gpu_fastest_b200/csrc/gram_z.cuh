@@ -7,8 +7,12 @@
 // contain z; this kernel computes each H(z) once and adds it into every active
 // window, which cuts the FFMA work by that factor (3.2x at 11^3 / stride 3).
 //
-// Layout: one CTA per (x-corner, y-corner) column, thread (bi, bj), bi <= bj,
-// owning the 4x4 block G[4bi:4bi+4, 4bj:4bj+4]. The column's planes are
+// Layout: one CTA per (x-corner, y-corner) column; ``ks`` adjacent threads
+// (lanes of one warp) share the 4x4 block G[4bi:4bi+4, 4bj:4bj+4], bi <= bj,
+// each summing every ks-th voxel row of a plane, combined by shuffles (a
+// K-split: ks times the warps per column for latency hiding). The block size
+// is rounded up to whole warps; the extra threads only join the shuffles and
+// barriers. The column's planes are
 // streamed into a two-slot shared-memory ring by TMA (one 4D box (T, 1, py, px)
 // of the centred volume per plane, completion on an mbarrier); the window
 // accumulators of the active windows live in shared memory (a ring of
@@ -79,46 +83,59 @@ __host__ __device__ inline size_t gramz_plane_floats(int rows, int T) {
   return ((size_t)rows * T + 31) & ~size_t(31);  // 128-byte multiple
 }
 
-// Dynamic shared memory: two plane slots, ring * 16 * nthreads float window
-// accumulators, two mbarriers.
-__host__ __device__ inline size_t gramz_smem_bytes(int rows, int T, int ring, int nthreads) {
-  return sizeof(float) * (2 * gramz_plane_floats(rows, T) + (size_t)ring * 16 * nthreads) + 16;
+// Dynamic shared memory: two plane slots, ring * 16 * nblk float window
+// accumulators (nblk = 4x4 blocks of the upper triangle), two mbarriers.
+__host__ __device__ inline size_t gramz_smem_bytes(int rows, int T, int ring, int nblk) {
+  return sizeof(float) * (2 * gramz_plane_floats(rows, T) + (size_t)ring * 16 * nblk) + 16;
 }
 
-// grid: (columns in this launch); block: nb*(nb+1)/2 threads, nb = T/4 (T % 4 == 0).
-// ``col0`` = first column (x-major index ci * ncy + cj); ``gram`` points at the
-// Gram block of the launch's first patch (patch index col0 * ncz).
-__global__ void gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g,
-                              AxisTables tab, long long col0, int ring, int* status) {
+// Threads of a column CTA for T frames and K-split ks: nb*(nb+1)/2 blocks
+// (nb = T/4) times ks, rounded up to whole warps.
+__host__ __device__ inline int gramz_threads(int T, int ks) {
+  const int nb = T >> 2;
+  return ((nb * (nb + 1) / 2 * ks) + 31) & ~31;
+}
+
+// grid: (columns in this launch); block: gramz_threads(T, ks) (T % 4 == 0,
+// ks in {1, 2, 4}). ``col0`` = first column (x-major index ci * ncy + cj);
+// ``gram`` points at the Gram block of the launch's first patch (patch index
+// col0 * ncz).
+__global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g,
+                              AxisTables tab, long long col0, int ring, int ks, int* status) {
   extern __shared__ __align__(128) float smz[];
   const int T = g.nt;
   const int rows = g.px * g.py;
   const size_t pf = gramz_plane_floats(rows, T);
   float* plane0 = smz;
   float* plane1 = smz + pf;
-  float* win = smz + 2 * pf;  // [ring][16][nthreads]
+  const int nb = T >> 2;
+  const int nblk = nb * (nb + 1) / 2;
+  float* win = smz + 2 * pf;  // [ring][16][nblk]
   const int nthreads = blockDim.x;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(win + (size_t)ring * 16 * nthreads);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(win + (size_t)ring * 16 * nblk);
   const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&bars[0]);
   const uint32_t bar1 = (uint32_t)__cvta_generic_to_shared(&bars[1]);
 
   const long long col = col0 + blockIdx.x;
   const int ci = (int)(col / g.ncy), cj = (int)(col % g.ncy);
   const int cx = tab.corners[0][ci], cy = tab.corners[1][cj];
-  const int nb = T >> 2;
   const int tid = threadIdx.x;
+  const int blk = tid / ks, kq = tid - (tid / ks) * ks;
+  const bool owner = blk < nblk;
   int bi = 0, bj = 0;
-  {
-    int rem = tid;
+  if (owner) {
+    int rem = blk;
     while (bi < nb && rem >= nb - bi) {
       rem -= nb - bi;
       ++bi;
     }
     bj = bi + rem;
   }
+  const int ucount = 16 / ks;      // window entries this thread updates
+  const int ubase = kq * ucount;
   const uint32_t plane_bytes = (uint32_t)(rows * T * sizeof(float));
 
-  for (int e = tid; e < ring * 16 * nthreads; e += nthreads) win[e] = 0.f;
+  for (int e = tid; e < ring * 16 * nblk; e += nthreads) win[e] = 0.f;
   if (tid == 0) {
     mbar_init(bar0, 1);
     mbar_init(bar1, 1);
@@ -148,7 +165,7 @@ __global__ void gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* _
       const float4* rp = reinterpret_cast<const float4*>(pl);
       const int ld4 = T >> 2;
 #pragma unroll 4
-      for (int r = 0; r < rows; ++r) {
+      for (int r = kq; r < rows; r += ks) {
         const float4 va = rp[r * ld4 + bi];
         const float4 vb = rp[r * ld4 + bj];
         const float a4[4] = {va.x, va.y, va.z, va.w};
@@ -158,24 +175,39 @@ __global__ void gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* _
 #pragma unroll
           for (int v = 0; v < 4; ++v) acc[u * 4 + v] = fmaf(a4[u], b4[v], acc[u * 4 + v]);
       }
-      for (int k = klo; k <= khi; ++k) {
-        float* w = win + (size_t)(k % ring) * 16 * nthreads + tid;
-        const bool last = z == tab.corners[2][k] + g.pz - 1;
-        if (!last) {
+      // combine the ks partial sums (every lane of the group ends with the total)
+      if (ks >= 2) {
 #pragma unroll
-          for (int u = 0; u < 16; ++u) w[u * nthreads] += acc[u];
-        } else {
-          float* G = G0 + (size_t)k * T * T;
+        for (int u = 0; u < 16; ++u) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 1);
+      }
+      if (ks >= 4) {
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 16; ++u) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 2);
+      }
+      if (owner) {
+        for (int k = klo; k <= khi; ++k) {
+          float* w = win + (size_t)(k % ring) * 16 * nblk + blk;
+          const bool last = z == tab.corners[2][k] + g.pz - 1;
+          if (!last) {
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-              const float val = w[(u * 4 + v) * nthreads] + acc[u * 4 + v];
-              w[(u * 4 + v) * nthreads] = 0.f;
-              const int r = bi * 4 + u, c = bj * 4 + v;
-              G[(size_t)r * T + c] = val;
-              G[(size_t)c * T + r] = val;
-            }
+            for (int u = 0; u < 16; ++u)
+              if (u >= ubase && u < ubase + ucount) w[u * nblk] += acc[u];
+          } else {
+            float* G = G0 + (size_t)k * T * T;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int v = 0; v < 4; ++v) {
+                const int e = u * 4 + v;
+                if (e >= ubase && e < ubase + ucount) {
+                  const float val = w[e * nblk] + acc[e];
+                  w[e * nblk] = 0.f;
+                  const int r = bi * 4 + u, c = bj * 4 + v;
+                  G[(size_t)r * T + c] = val;
+                  G[(size_t)c * T + r] = val;
+                }
+              }
+          }
         }
       }
     }

@@ -72,6 +72,7 @@ struct lrd_plan {
   bool use_gramtc;         // the column Gram on tcgen05 (tensor form)
   size_t smem_gramtc;
   int gramz_ring;          // window accumulator slots
+  int gramz_ks = 1;        // voxel-row split per 4x4 Gram block (threads per block)
   size_t smem_gramz;
   size_t smem_center, smem_gram, smem_eigh, smem_recon;
   int center_warps;
@@ -85,7 +86,9 @@ struct lrd_plan {
   // host copies of the x-axis tables (host-buffer pipeline) and its streams/events
   std::vector<int32_t> h_corner_x, h_brick_x;
   cudaStream_t io_in = nullptr, io_out = nullptr;
-  std::vector<cudaEvent_t> io_events;  // 2 per slab + 1
+  cudaStream_t io_prep[3] = {nullptr, nullptr, nullptr};  // centre + Gram of slab s on io_prep[s % 3]
+  cudaStream_t io_recon = nullptr;                         // reconstruction of the slabs
+  std::vector<cudaEvent_t> io_events;  // 5 per slab + 1
   // measurement hook: a ring of per-call phase events
   bool profiling = false;
   int prof_calls = 0;
@@ -99,10 +102,19 @@ struct lrd_plan {
 
 namespace {
 constexpr int kProfRing = 256;
-constexpr int kIoSlabs = 8;  // x-slabs of the host-buffer pipeline
+constexpr int kIoSlabs = 16;     // event capacity of the host-buffer pipeline
+// x-slabs the host-buffer pipeline uses. Measured e2e at 96x96x48x48 / 11^3 /
+// stride 3 on B200 (ms): 4 slabs 4.73, 6 4.74, 8 4.62, 10 4.55, 12 4.62, 16 5.05.
+constexpr int kIoSlabsUsed = 10;
 }
 
 namespace {
+
+// Voxel-row split of the column Gram. Measured on B200 (96x96x48xT, 11^3,
+// stride 3): T = 48 runs 0.80 ms with 2 threads per block (160-thread CTAs)
+// against 0.96 ms unsplit and 1.27 ms with 4; T = 32, 64 and 96 are fastest
+// unsplit (0.58 / 1.44 / 1.21 ms, the split costing 30-60%).
+int gramz_split(int T) { return (T > 40 && T <= 56) ? 2 : 1; }
 
 // Reconstruction thread layout for T frames: two threads per voxel up to
 // T = 96 (one shuffle per eigenvector; one thread per voxel needs ~220
@@ -327,8 +339,8 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
                                                                       P->tab, c0, P->gramz_ring, status);
         rc = launch_check("gram_tc_kernel launch");
       } else {
-        lrd::gram_z_kernel<<<(unsigned)nc, P->gram_threads, P->smem_gramz, st>>>(
-            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, status);
+        lrd::gram_z_kernel<<<(unsigned)nc, lrd::gramz_threads(P->g.nt, P->gramz_ks), P->smem_gramz, st>>>(
+            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, P->gramz_ks, status);
         rc = launch_check("gram_z_kernel launch");
       }
       if (rc) return rc;
@@ -568,6 +580,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     int ring = 1;
     for (int z = 0; z < pr->nz; ++z) ring = std::max(ring, cover[2][2 * z + 1] - cover[2][2 * z] + 1);
     P->gramz_ring = ring;
+    P->gramz_ks = gramz_split(T);
     P->smem_gramz = lrd::gramz_smem_bytes(pr->px * pr->py, T, ring, P->gram_threads);
     P->use_gramz = (T % 4 == 0) && P->smem_gramz <= 200 * 1024 && tensor_map_encoder() != nullptr &&
                    pr->px <= 256 && pr->py <= 256;
@@ -607,11 +620,18 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   {
     cudaError_t e1 = cudaStreamCreateWithFlags(&P->io_in, cudaStreamNonBlocking);
     cudaError_t e2 = cudaStreamCreateWithFlags(&P->io_out, cudaStreamNonBlocking);
+    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_recon}) {
+      cudaError_t e4 = cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking);
+      if (e4 != cudaSuccess) {
+        *ps = nullptr;
+        if (e1 == cudaSuccess) e1 = e4;
+      }
+    }
     if (e1 != cudaSuccess || e2 != cudaSuccess) {
       lrd_plan_destroy(P);
       return cuda_fail(e1 != cudaSuccess ? e1 : e2, "cudaStreamCreateWithFlags");
     }
-    P->io_events.resize(2 * kIoSlabs + 1);
+    P->io_events.resize(5 * kIoSlabs + 1);
     for (auto& ev : P->io_events) {
       cudaError_t e3 = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
       if (e3 != cudaSuccess) {
@@ -710,6 +730,9 @@ int lrd_plan_destroy(lrd_plan* P) {
     if (e) cudaEventDestroy(e);
   if (P->io_in) cudaStreamDestroy(P->io_in);
   if (P->io_out) cudaStreamDestroy(P->io_out);
+  for (auto ps : P->io_prep)
+    if (ps) cudaStreamDestroy(ps);
+  if (P->io_recon) cudaStreamDestroy(P->io_recon);
   if (P->d_tables) cudaFree(P->d_tables);
   delete P;
   return LRD_OK;
@@ -768,12 +791,16 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   if (!h_vol || !h_out || !d_in || !d_out || !d_ws) return fail(LRD_ERR_INVALID, "NULL buffer");
   if (h_ranks && !d_ranks) return fail(LRD_ERR_INVALID, "h_ranks needs d_ranks");
   if (reinterpret_cast<uintptr_t>(d_ws) % 256) return fail(LRD_ERR_INVALID, "workspace not 256-byte aligned");
-  // Pipeline over x-slabs of patch corners: slab s copies in the x-planes its
-  // patch columns need (copy-in stream), centres them, forms and solves those
-  // columns' patches and refines their near-ties, reconstructs the bricks
-  // whose touching patches are now all final (compute stream = ``stream``),
-  // and copies those bricks' output planes back (copy-out stream). Copies of
-  // one slab overlap the compute of its neighbours.
+  // Pipeline over x-slabs of patch corners. Slab s: copy in the x-planes its
+  // patch columns need (copy-in stream); centre them and form those columns'
+  // Gram matrices on io_prep[s % 3] (a slab's Gram launch is a fraction of a
+  // wave, so three slabs' Grams run side by side); solve the slab's patches,
+  // refine their near-ties on the compute stream ``stream``; reconstruct the
+  // bricks whose touching patches are now all final on the reconstruction
+  // stream (overlapping the next slab's solve); copy those bricks' output
+  // planes back (copy-out stream). Events order: copy-in(s) -> centre(s)
+  // (after centre(s - 1), whose planes the slab's columns share) -> Gram(s)
+  // -> solve(s) -> reconstruct(s) -> copy-out(s).
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   char* ws = static_cast<char*>(d_ws);
   const lrd::Geom& g = P->g;
@@ -782,48 +809,59 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   float* gv = reinterpret_cast<float*>(ws + P->off_gv);
   int32_t* rank = reinterpret_cast<int32_t*>(ws + P->off_rank);
   float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
-  cudaEvent_t start = P->io_events[2 * kIoSlabs];
+  // k: 0 copied in, 1 centred, 2 Gram, 3 reconstructed, 4 solved
+  auto ev = [&](int s, int k) { return P->io_events[5 * s + k]; };
+  cudaEvent_t start = P->io_events[5 * kIoSlabs];
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 2 * sizeof(int32_t), st));
   LRD_CUDA(cudaEventRecord(start, st));
   LRD_CUDA(cudaStreamWaitEvent(P->io_in, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_out, start, 0));
-  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
-  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 2 * sizeof(int32_t), st));
-  const int S = std::max(1, std::min(kIoSlabs, g.ncx));
+  for (auto ps : P->io_prep) LRD_CUDA(cudaStreamWaitEvent(ps, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
+  const int S = std::max(1, std::min(kIoSlabsUsed, g.ncx));
   int planes_in = 0, ci_done = 0, bx_done = 0;
   const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
   for (int s = 0; s < S; ++s) {
     const int ci_end = (int)((long long)(s + 1) * g.ncx / S);
     const bool lastslab = s == S - 1;
     const int x_need = lastslab ? g.nx : std::min(g.nx, P->h_corner_x[ci_end - 1] + g.px);
-    cudaEvent_t ev_in = P->io_events[2 * s], ev_done = P->io_events[2 * s + 1];
+    cudaStream_t prep = P->io_prep[s % 3];
     if (x_need > planes_in)
       LRD_CUDA(cudaMemcpyAsync(d_in + planes_in * plane, h_vol + planes_in * plane,
                                sizeof(float) * (size_t)(x_need - planes_in) * plane, cudaMemcpyHostToDevice,
                                P->io_in));
-    LRD_CUDA(cudaEventRecord(ev_in, P->io_in));
-    LRD_CUDA(cudaStreamWaitEvent(st, ev_in, 0));
-    if ((rc = run_center(P, d_in, ws, st, planes_in * plane_vox, (long long)(x_need - planes_in) * plane_vox)))
+    LRD_CUDA(cudaEventRecord(ev(s, 0), P->io_in));
+    LRD_CUDA(cudaStreamWaitEvent(prep, ev(s, 0), 0));
+    if (s > 0) LRD_CUDA(cudaStreamWaitEvent(prep, ev(s - 1, 1), 0));
+    if ((rc = run_center(P, d_in, ws, prep, planes_in * plane_vox, (long long)(x_need - planes_in) * plane_vox)))
       return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 1), prep));
     planes_in = std::max(planes_in, x_need);
-    if ((rc = run_gram(P, ws, gv, st, ci_done * colz, ci_end * colz))) return rc;
+    if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz))) return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
+    LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
     if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false))) return rc;
     ci_done = ci_end;
     int bx_end = bx_done;
     while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
-    if ((rc = run_recon(P, ws, d_out, st, bx_done * brz, bx_end * brz))) return rc;
-    LRD_CUDA(cudaEventRecord(ev_done, st));
+    LRD_CUDA(cudaEventRecord(ev(s, 4), st));
+    LRD_CUDA(cudaStreamWaitEvent(P->io_recon, ev(s, 4), 0));
+    if ((rc = run_recon(P, ws, d_out, P->io_recon, bx_done * brz, bx_end * brz))) return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 3), P->io_recon));
     if (bx_end > bx_done) {
       const long long x0 = (long long)bx_done * g.bx, x1 = std::min<long long>((long long)bx_end * g.bx, g.nx);
-      LRD_CUDA(cudaStreamWaitEvent(P->io_out, ev_done, 0));
+      LRD_CUDA(cudaStreamWaitEvent(P->io_out, ev(s, 3), 0));
       LRD_CUDA(cudaMemcpyAsync(h_out + x0 * plane, d_out + x0 * plane, sizeof(float) * (size_t)(x1 - x0) * plane,
                                cudaMemcpyDeviceToHost, P->io_out));
     }
     bx_done = bx_end;
   }
+  LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 1, 3), 0));  // the last reconstruction joins the caller's stream
   if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * g.npatch, cudaMemcpyDeviceToDevice, st));
   if (h_ranks) {
-    LRD_CUDA(cudaEventRecord(P->io_events[2 * S - 1], st));
-    LRD_CUDA(cudaStreamWaitEvent(P->io_out, P->io_events[2 * S - 1], 0));
+    LRD_CUDA(cudaEventRecord(ev(S - 1, 4), st));
+    LRD_CUDA(cudaStreamWaitEvent(P->io_out, ev(S - 1, 4), 0));
     LRD_CUDA(cudaMemcpyAsync(h_ranks, d_ranks, sizeof(int32_t) * g.npatch, cudaMemcpyDeviceToHost, P->io_out));
   }
   LRD_CUDA(cudaStreamSynchronize(P->io_out));
