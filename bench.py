@@ -593,7 +593,7 @@ def run_serving(args):
     from lowrank_gpu_fastest_b200.serve import Server, draw_request_shapes, poisson_arrivals
 
     shapes = draw_request_shapes(args.requests, seed=args.seed, big_fraction=0.1)
-    arr = poisson_arrivals(args.rate, 1e9, seed=args.seed)[: args.requests]
+    arr = poisson_arrivals(args.rate, float("inf"), seed=args.seed, max_count=args.requests)
     vols = [make_phantom_lowrank(r["shape"], seed=i, sigma=r["sigma"])[0] for i, r in enumerate(shapes)]
     # warm: plans and one solve per distinct problem
     seen = set()

@@ -48,6 +48,109 @@ __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
   return (size_t)TMAX * TMAX + 2 * TMAX + 5 * TMAX + (size_t)4 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
 }
 
+// Sturm counts (eigenvalues below x0 and x1) of the tridiagonal held in
+// registers: dr[i] = d_i, e2r[i] = e_i^2. Entries i >= n are padded with
+// d_i = +big, e_i = 0, which adds positive pivots only, so the counts equal
+// the n x n ones; for i < n the arithmetic is sturm_count2's.
+template <int TMAX>
+__device__ __forceinline__ void sturm2_reg(const float (&dr)[TMAX], const float (&e2r)[TMAX], float x0, float x1,
+                                           float pivmin, int& c0, int& c1) {
+  float q0 = dr[0] - x0, q1 = dr[0] - x1;
+  if (fabsf(q0) < pivmin) q0 = -pivmin;
+  if (fabsf(q1) < pivmin) q1 = -pivmin;
+  int a0 = q0 < 0.f, a1 = q1 < 0.f;
+#pragma unroll
+  for (int i = 1; i < TMAX; ++i) {
+    q0 = (dr[i] - x0) - __fdividef(e2r[i - 1], q0);
+    q1 = (dr[i] - x1) - __fdividef(e2r[i - 1], q1);
+    if (fabsf(q0) < pivmin) q0 = -pivmin;
+    if (fabsf(q1) < pivmin) q1 = -pivmin;
+    a0 += q0 < 0.f;
+    a1 += q1 < 0.f;
+  }
+  c0 = a0;
+  c1 = a1;
+}
+
+// All eigenvalues of the tridiagonal (d, e, e2 in shared memory) ascending
+// into lam; tnorm = Gerschgorin bound. bisect_all's bisection (same interval
+// rule and stopping test) with the tridiagonal in registers and one
+// multisection pass first: the 64 chains evaluate counts at 64 evenly spaced
+// interior points of the Gerschgorin interval, and every chain starts from
+// the two neighbouring points that bracket its eigenvalue (six bisection
+// steps for the price of one).
+template <int TMAX>
+__device__ __forceinline__ void bisect_reg(const float* d, const float* e, const float* e2, float* lam, int n,
+                                           float& tnorm_out) {
+  const int lane = threadIdx.x & 31;
+  const float eps = Num<float>::eps();
+  float glo = FLT_MAX, ghi = -FLT_MAX;
+  for (int i = lane; i < n; i += 32) {
+    const float r = (i > 0 ? fabsf(e[i - 1]) : 0.f) + (i < n - 1 ? fabsf(e[i]) : 0.f);
+    glo = fminf(glo, d[i] - r);
+    ghi = fmaxf(ghi, d[i] + r);
+  }
+  glo = warp_min(glo);
+  ghi = warp_max(ghi);
+  const float tnorm = fmaxf(fmaxf(fabsf(glo), fabsf(ghi)), FLT_MIN);
+  glo -= 4.f * eps * tnorm * n;
+  ghi += 4.f * eps * tnorm * n;
+  const float pivmin = FLT_MIN * 4.f;
+  const float abstol = 0.1f * eps * tnorm;
+  const float big = 4.f * fmaxf(fabsf(glo), fabsf(ghi)) + 1.f;
+  float dr[TMAX], e2r[TMAX];
+#pragma unroll
+  for (int i = 0; i < TMAX; ++i) {
+    dr[i] = i < n ? d[i] : big;
+    e2r[i] = i < n - 1 ? e2[i] : 0.f;
+  }
+  // multisection: counts at y_m = glo + (m + 1) h, m = lane and lane + 32
+  const float h = (ghi - glo) * (1.f / 65.f);
+  int cm0, cm1;
+  sturm2_reg<TMAX>(dr, e2r, fmaf((float)(lane + 1), h, glo), fmaf((float)(lane + 33), h, glo), pivmin, cm0, cm1);
+  const int j0 = lane, j1 = lane + 32;
+  float lo0 = glo, hi0 = ghi, lo1 = glo, hi1 = ghi;
+#pragma unroll 4
+  for (int m = 0; m < 32; ++m) {
+    const int ca = __shfl_sync(0xffffffffu, cm0, m), cb = __shfl_sync(0xffffffffu, cm1, m);
+    const float ya = fmaf((float)(m + 1), h, glo), yb = fmaf((float)(m + 33), h, glo);
+    if (ca <= j0) lo0 = fmaxf(lo0, ya); else hi0 = fminf(hi0, ya);
+    if (cb <= j0) lo0 = fmaxf(lo0, yb); else hi0 = fminf(hi0, yb);
+    if (ca <= j1) lo1 = fmaxf(lo1, ya); else hi1 = fminf(hi1, ya);
+    if (cb <= j1) lo1 = fmaxf(lo1, yb); else hi1 = fminf(hi1, yb);
+  }
+  if (!(lo0 < hi0)) { lo0 = glo; hi0 = ghi; }  // counts not monotone: full interval
+  if (!(lo1 < hi1)) { lo1 = glo; hi1 = ghi; }
+  const bool has0 = j0 < n, has1 = j1 < n;
+  bool run0 = has0, run1 = has1;
+  for (int it = 0; it < 200 && (run0 || run1); ++it) {
+    if (run0) {
+      const float tol = fmaxf(abstol, 2.f * eps * fmaxf(fabsf(lo0), fabsf(hi0)));
+      const float mid = 0.5f * (lo0 + hi0);
+      run0 = hi0 - lo0 > tol && mid > lo0 && mid < hi0;
+    }
+    if (run1) {
+      const float tol = fmaxf(abstol, 2.f * eps * fmaxf(fabsf(lo1), fabsf(hi1)));
+      const float mid = 0.5f * (lo1 + hi1);
+      run1 = hi1 - lo1 > tol && mid > lo1 && mid < hi1;
+    }
+    if (!run0 && !run1) break;
+    const float m0 = 0.5f * (lo0 + hi0), m1 = 0.5f * (lo1 + hi1);
+    int c0, c1;
+    sturm2_reg<TMAX>(dr, e2r, m0, m1, pivmin, c0, c1);
+    if (run0) {
+      if (c0 > j0) hi0 = m0; else lo0 = m0;
+    }
+    if (run1) {
+      if (c1 > j1) hi1 = m1; else lo1 = m1;
+    }
+  }
+  if (has0) lam[j0] = 0.5f * (lo0 + hi0);
+  if (has1) lam[j1] = 0.5f * (lo1 + hi1);
+  __syncwarp();
+  tnorm_out = tnorm;
+}
+
 template <int TMAX>
 __global__ void __launch_bounds__(32)
     eigh_reg_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
@@ -144,22 +247,30 @@ __global__ void __launch_bounds__(32)
     }
     __syncwarp();
     if (taui != 0.f) {
-      // p = taui * A22 v over own rows (columns j >= k+1; hv is 0 below)
+      // p = taui * A22 v over own rows (columns j >= k+1; hv is 0 below).
+      // The column groups j4 < j4lo are dead: a switch on j4lo enters the
+      // unrolled groups at the first live one (cases fall through), so the
+      // register indices stay compile-time and the dead groups cost nothing.
       const int j4lo = (k + 1) >> 2;
       float pr[NR];
 #pragma unroll
       for (int ri = 0; ri < NR; ++ri) {
         float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
-#pragma unroll
-        for (int j4 = 0; j4 < TMAX / 4; ++j4) {
-          if (j4 >= j4lo) {
-            const float4 v4 = reinterpret_cast<const float4*>(hv)[j4];
-            s0 = fmaf(a[ri][4 * j4 + 0], v4.x, s0);
-            s1 = fmaf(a[ri][4 * j4 + 1], v4.y, s1);
-            s2 = fmaf(a[ri][4 * j4 + 2], v4.z, s2);
-            s3 = fmaf(a[ri][4 * j4 + 3], v4.w, s3);
-          }
+#define LRD_MV(J)                                                   \
+  case J:                                                           \
+    if constexpr (J < TMAX / 4) {                                   \
+      const float4 v4 = reinterpret_cast<const float4*>(hv)[J];     \
+      s0 = fmaf(a[ri][4 * J + 0], v4.x, s0);                        \
+      s1 = fmaf(a[ri][4 * J + 1], v4.y, s1);                        \
+      s2 = fmaf(a[ri][4 * J + 2], v4.z, s2);                        \
+      s3 = fmaf(a[ri][4 * J + 3], v4.w, s3);                        \
+    }
+        switch (j4lo) {
+          LRD_MV(0) LRD_MV(1) LRD_MV(2) LRD_MV(3) LRD_MV(4) LRD_MV(5) LRD_MV(6) LRD_MV(7)
+          LRD_MV(8) LRD_MV(9) LRD_MV(10) LRD_MV(11) LRD_MV(12) LRD_MV(13) LRD_MV(14) LRD_MV(15)
+          default: break;
         }
+#undef LRD_MV
         const int r = lane + 32 * ri;
         pr[ri] = (r >= k + 1 && r < n) ? taui * ((s0 + s1) + (s2 + s3)) : 0.f;
       }
@@ -175,20 +286,26 @@ __global__ void __launch_bounds__(32)
         if (r < TMAX) ws[r] = wr[ri];
       }
       __syncwarp();
-      // A22 -= v w^T + w v^T on own rows, columns j >= k+1 (ws, hv zero below)
+      // A22 -= v w^T + w v^T on own rows, columns j >= k+1 (ws, hv zero
+      // below), live column groups only as above
 #pragma unroll
       for (int ri = 0; ri < NR; ++ri) {
-#pragma unroll
-        for (int j4 = 0; j4 < TMAX / 4; ++j4) {
-          if (j4 >= j4lo) {
-            const float4 v4 = reinterpret_cast<const float4*>(hv)[j4];
-            const float4 w4 = reinterpret_cast<const float4*>(ws)[j4];
-            a[ri][4 * j4 + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * j4 + 0]));
-            a[ri][4 * j4 + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * j4 + 1]));
-            a[ri][4 * j4 + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * j4 + 2]));
-            a[ri][4 * j4 + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * j4 + 3]));
-          }
+#define LRD_UPD(J)                                                                   \
+  case J:                                                                            \
+    if constexpr (J < TMAX / 4) {                                                    \
+      const float4 v4 = reinterpret_cast<const float4*>(hv)[J];                      \
+      const float4 w4 = reinterpret_cast<const float4*>(ws)[J];                      \
+      a[ri][4 * J + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * J + 0])); \
+      a[ri][4 * J + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * J + 1])); \
+      a[ri][4 * J + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * J + 2])); \
+      a[ri][4 * J + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * J + 3])); \
+    }
+        switch (j4lo) {
+          LRD_UPD(0) LRD_UPD(1) LRD_UPD(2) LRD_UPD(3) LRD_UPD(4) LRD_UPD(5) LRD_UPD(6) LRD_UPD(7)
+          LRD_UPD(8) LRD_UPD(9) LRD_UPD(10) LRD_UPD(11) LRD_UPD(12) LRD_UPD(13) LRD_UPD(14) LRD_UPD(15)
+          default: break;
         }
+#undef LRD_UPD
       }
     }
     __syncwarp();  // xk, ws are rewritten by the next step
@@ -199,7 +316,7 @@ __global__ void __launch_bounds__(32)
   LRD_STAMP(2);
   // ---- eigenvalues, MP rank ---------------------------------------------------
   float tnorm;
-  bisect_all<float>(d, e, e2, lam, n, tnorm);
+  bisect_reg<TMAX>(d, e, e2, lam, n, tnorm);
   LRD_STAMP(3);
   int p;
   const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p);
@@ -229,28 +346,21 @@ __global__ void __launch_bounds__(32)
       const float sig = lam[n - 1 - j];
       // LU with partial pivoting of (T - sig I)
       float c = d[0] - sig, s = (n > 1) ? e[0] : 0.f;
+      // (the lanes pivot differently: selects, not branches)
       for (int i = 0; i < n - 1; ++i) {
         const float ei = e[i];
         const float an = d[i + 1] - sig;
         const float en = (i + 1 < n - 1) ? e[i + 1] : 0.f;
-        float piv;
-        if (fabsf(c) >= fabsf(ei)) {
-          const float m = (ei == 0.f) ? 0.f : __fdividef(ei, c);
-          piv = c;
-          U1[i * kInvGroup + q] = s;
-          ML[i * kInvGroup + q] = m;
-          SW[i * kInvGroup + q] = 0.f;
-          c = fmaf(-m, s, an);
-          s = en;
-        } else {
-          const float m = __fdividef(c, ei);
-          piv = ei;
-          U1[i * kInvGroup + q] = an;
-          ML[i * kInvGroup + q] = m;
-          SW[i * kInvGroup + q] = 1.f;
-          c = fmaf(-m, an, s);
-          s = -m * en;
-        }
+        const bool keep = fabsf(c) >= fabsf(ei);
+        const float num = keep ? ei : c, den = keep ? c : ei;
+        const float m = (keep && ei == 0.f) ? 0.f : __fdividef(num, den);
+        float piv = den;
+        U1[i * kInvGroup + q] = keep ? s : an;
+        ML[i * kInvGroup + q] = m;
+        SW[i * kInvGroup + q] = keep ? 0.f : 1.f;
+        const float cn = keep ? fmaf(-m, s, an) : fmaf(-m, an, s);
+        s = keep ? en : -m * en;
+        c = cn;
         if (fabsf(piv) < pivtol) piv = (piv < 0.f) ? -pivtol : pivtol;
         RU0[i * kInvGroup + q] = __fdividef(1.f, piv);
       }
@@ -264,13 +374,10 @@ __global__ void __launch_bounds__(32)
         for (int i = 0; i < TMAX - 1; ++i) {
           if (i < n - 1) {
             const float m = ML[i * kInvGroup + q];
-            if (SW[i * kInvGroup + q] != 0.f) {
-              const float bi = y[i];
-              y[i] = y[i + 1];
-              y[i + 1] = fmaf(-m, y[i + 1], bi);
-            } else {
-              y[i + 1] = fmaf(-m, y[i], y[i + 1]);
-            }
+            const bool sw = SW[i * kInvGroup + q] != 0.f;
+            const float yi = y[i], yn = y[i + 1];
+            y[i] = sw ? yn : yi;
+            y[i + 1] = sw ? fmaf(-m, yn, yi) : fmaf(-m, yi, yn);
           }
         }
         float amax = 0.f;

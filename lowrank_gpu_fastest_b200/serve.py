@@ -231,15 +231,17 @@ class Server:
             time.sleep(self.poll_s)
 
 
-def poisson_arrivals(rate_per_s, duration_s, seed=0):
-    """Arrival times (s) of a Poisson process, seeded."""
+def poisson_arrivals(rate_per_s, duration_s, seed=0, max_count=None):
+    """Arrival times (s) of a Poisson process, seeded: those before
+    ``duration_s``, at most ``max_count`` of them."""
     rng = np.random.default_rng(seed)
     t, out = 0.0, []
-    while True:
+    while max_count is None or len(out) < max_count:
         t += rng.exponential(1.0 / rate_per_s)
         if t >= duration_s:
-            return np.array(out)
+            break
         out.append(t)
+    return np.array(out)
 
 
 def draw_request_shapes(n, seed=0, big_fraction=0.1, t_choices=(32, 48, 64, 96)):
