@@ -508,10 +508,335 @@ __global__ void __launch_bounds__(32)
   }
 }
 
+// One CTA of 128 threads: the same decomposition as eigh_mp_warp<Real> for
+// the float64 pass at T > 64, where one warp per matrix leaves a near-tie's
+// refinement (a single wave of such solves) far behind the main pass. The
+// matrix stays in shared memory (odd row stride: a warp's threads, one row
+// each, hit distinct banks); thread i owns row i of the trailing block in the
+// Householder steps, the two dot products per step are block reductions;
+// thread j bisects eigenvalue j; inverse iteration (one lane per vector),
+// the back-transform (warp w: vectors w and w + 4) and Gram-Schmidt follow
+// eigh_mp_warp. ``red`` = 8 elements of scratch. Returns the MP margin (all
+// threads).
+template <typename Real>
+__device__ Real block_sum128(Real v, Real* red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  return (red[0] + red[1]) + (red[2] + red[3]);
+}
+
+template <typename Real>
+__device__ Real block_max128(Real v, Real* red) {
+  v = warp_max(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  return fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
+}
+
+template <typename Real>
+__device__ Real block_min128(Real v, Real* red) {
+  v = warp_min(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  return fmin(fmin(red[0], red[1]), fmin(red[2], red[3]));
+}
+
+template <typename Real>
+__device__ __forceinline__ int sturm_count1_r(const Real* d, const Real* e2, int n, Real x, Real pivmin) {
+  Real q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int a = q < Real(0);
+  for (int i = 1; i < n; ++i) {
+    q = (d[i] - x) - Num<Real>::fdiv(e2[i - 1], q);
+    if (fabs(q) < pivmin) q = -pivmin;
+    a += q < Real(0);
+  }
+  return a;
+}
+
+template <typename Real>
+__device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, float* lam_out, int32_t* rank_out,
+                                float* w_out) {
+  constexpr int NT = 128;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int lda = eigh_lda(n);
+  Real* A = sm;
+  Real* Y = A + n * lda;
+  Real* d = Y + n * kLdy;
+  Real* e = d + n;
+  Real* e2 = e + n;
+  Real* tau = e2 + n;
+  Real* lam = tau + n;
+  Real* W = lam + n;
+  const Real eps = Num<Real>::eps();
+
+  Real dm = 0;
+  for (int i = tid; i < n; i += NT) dm = fmax(dm, fabs(A[i * lda + i]));
+  dm = block_max128(dm, red);
+  int ex = 0;
+  if (dm > Real(0) && isfinite(dm)) frexp(dm, &ex);
+  const Real scale = ldexp(Real(1), -ex), unscale = ldexp(Real(1), ex);
+  for (int idx = tid; idx < n * n; idx += NT) {
+    const int r = idx / n, c = idx - r * n;
+    A[r * lda + c] *= scale;
+  }
+  __syncthreads();
+
+  Real* vv = W;
+  Real* pp = W + n;
+  Real* ww = W + 2 * n;
+  for (int k = 0; k < n - 2; ++k) {
+    const int L = n - k - 1;
+    Real part = 0;
+    for (int i = 1 + tid; i < L; i += NT) {
+      const Real v = A[(k + 1 + i) * lda + k];
+      part = fma(v, v, part);
+    }
+    const Real xnorm2 = block_sum128(part, red);
+    const Real alpha = A[(k + 1) * lda + k];
+    Real taui = 0, beta = alpha, scv = 0;
+    if (xnorm2 > Real(0)) {
+      beta = -copysign(sqrt(fma(alpha, alpha, xnorm2)), alpha);
+      taui = (beta - alpha) / beta;
+      scv = Real(1) / (alpha - beta);
+    }
+    for (int i = tid; i < L; i += NT) {
+      if (i == 0) {
+        vv[0] = Real(1);
+      } else if (xnorm2 > Real(0)) {
+        const Real v = A[(k + 1 + i) * lda + k] * scv;
+        A[(k + 1 + i) * lda + k] = v;
+        vv[i] = v;
+      }
+    }
+    if (tid == 0) {
+      e[k] = beta;
+      d[k] = A[k * lda + k];
+      tau[k] = taui;
+    }
+    __syncthreads();
+    if (taui != Real(0)) {
+      for (int i = tid; i < L; i += NT) {
+        const Real* row = A + (k + 1 + i) * lda + (k + 1);
+        Real s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int j = 0;
+        for (; j + 4 <= L; j += 4) {
+          s0 = fma(row[j], vv[j], s0);
+          s1 = fma(row[j + 1], vv[j + 1], s1);
+          s2 = fma(row[j + 2], vv[j + 2], s2);
+          s3 = fma(row[j + 3], vv[j + 3], s3);
+        }
+        for (; j < L; ++j) s0 = fma(row[j], vv[j], s0);
+        pp[i] = taui * ((s0 + s1) + (s2 + s3));
+      }
+      __syncthreads();
+      Real part2 = 0;
+      for (int i = tid; i < L; i += NT) part2 = fma(pp[i], vv[i], part2);
+      const Real kc = Real(-0.5) * taui * block_sum128(part2, red);
+      for (int i = tid; i < L; i += NT) ww[i] = fma(kc, vv[i], pp[i]);
+      __syncthreads();
+      for (int i = tid; i < L; i += NT) {
+        const Real vi = vv[i], wi = ww[i];
+        Real* row = A + (k + 1 + i) * lda + (k + 1);
+        for (int j = 0; j < L; ++j) row[j] = fma(-vi, ww[j], fma(-wi, vv[j], row[j]));
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (n >= 2) {
+      d[n - 2] = A[(n - 2) * lda + (n - 2)];
+      e[n - 2] = A[(n - 1) * lda + (n - 2)];
+      tau[n - 2] = 0;
+    }
+    d[n - 1] = A[(n - 1) * lda + (n - 1)];
+    e[n - 1] = 0;
+    tau[n - 1] = 0;
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += NT) e2[i] = (i < n - 1) ? e[i] * e[i] : Real(0);
+  __syncthreads();
+
+  // bisection, thread j = eigenvalue j (bisect_all's interval rule and stopping test)
+  Real tnorm;
+  {
+    Real glo = Num<Real>::huge(), ghi = -Num<Real>::huge();
+    for (int i = tid; i < n; i += NT) {
+      const Real r = (i > 0 ? fabs(e[i - 1]) : Real(0)) + (i < n - 1 ? fabs(e[i]) : Real(0));
+      glo = fmin(glo, d[i] - r);
+      ghi = fmax(ghi, d[i] + r);
+    }
+    glo = block_min128(glo, red);
+    ghi = block_max128(ghi, red);
+    tnorm = fmax(fmax(fabs(glo), fabs(ghi)), Num<Real>::tiny());
+    glo -= Real(4) * eps * tnorm * n;
+    ghi += Real(4) * eps * tnorm * n;
+    const Real pivmin = Num<Real>::tiny() * Real(4);
+    const Real abstol = Real(0.1) * eps * tnorm;
+    for (int j = tid; j < n; j += NT) {
+      Real lo = glo, hi = ghi;
+      for (int it = 0; it < 200; ++it) {
+        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo), fabs(hi)));
+        const Real mid = Real(0.5) * (lo + hi);
+        if (!(hi - lo > tol && mid > lo && mid < hi)) break;
+        if (sturm_count1_r(d, e2, n, mid, pivmin) > j) hi = mid; else lo = mid;
+      }
+      lam[j] = Real(0.5) * (lo + hi);
+    }
+  }
+  __syncthreads();
+
+  int* pshare = reinterpret_cast<int*>(red + 4);
+  double margin = 0.0;
+  if (warp == 0) {
+    int p;
+    margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p);
+    if (lane == 0) {
+      *rank_out = p;
+      *w_out = (float)(1.0 / (2.0 + (double)p));
+      *pshare = p;
+    }
+  }
+  if (lam_out != nullptr)
+    for (int i = tid; i < n; i += NT) lam_out[i] = (float)(lam[i] * unscale);
+  __syncthreads();
+  const int p = *pshare;
+  if (p == 0) return margin;
+
+  const Real pivtol = eps * tnorm;
+  Real* RU0 = W;
+  Real* U1 = RU0 + n * kInvGroup;
+  Real* ML = U1 + n * kInvGroup;
+  Real* SW = ML + n * kInvGroup;
+  for (int j0 = 0; j0 < p; j0 += kInvGroup) {
+    const int g = min(kInvGroup, p - j0);
+    __syncthreads();
+    if (warp == 0 && lane < g) {
+      const int q = lane;
+      const int j = j0 + q;
+      const Real sig = lam[n - 1 - j];
+      Real c = d[0] - sig, s = (n > 1) ? e[0] : Real(0);
+      for (int i = 0; i < n - 1; ++i) {
+        const Real ei = e[i];
+        const Real an = d[i + 1] - sig;
+        const Real en = (i + 1 < n - 1) ? e[i + 1] : Real(0);
+        const bool keep = fabs(c) >= fabs(ei);
+        const Real m = keep ? ((ei == Real(0)) ? Real(0) : ei / c) : c / ei;
+        Real piv = keep ? c : ei;
+        U1[i * kInvGroup + q] = keep ? s : an;
+        ML[i * kInvGroup + q] = m;
+        SW[i * kInvGroup + q] = keep ? Real(0) : Real(1);
+        const Real cn = keep ? fma(-m, s, an) : fma(-m, an, s);
+        s = keep ? en : -m * en;
+        c = cn;
+        if (fabs(piv) < pivtol) piv = (piv < Real(0)) ? -pivtol : pivtol;
+        RU0[i * kInvGroup + q] = Real(1) / piv;
+      }
+      if (fabs(c) < pivtol) c = (c < Real(0)) ? -pivtol : pivtol;
+      RU0[(n - 1) * kInvGroup + q] = Real(1) / c;
+      for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
+      for (int iter = 0; iter < 3; ++iter) {
+        for (int i = 0; i < n - 1; ++i) {
+          const Real yi = Y[i * kLdy + q], yn = Y[(i + 1) * kLdy + q];
+          const Real m = ML[i * kInvGroup + q];
+          const bool sw = SW[i * kInvGroup + q] != Real(0);
+          Y[i * kLdy + q] = sw ? yn : yi;
+          Y[(i + 1) * kLdy + q] = sw ? fma(-m, yn, yi) : fma(-m, yi, yn);
+        }
+        Real x2 = Y[(n - 1) * kLdy + q] * RU0[(n - 1) * kInvGroup + q];
+        Y[(n - 1) * kLdy + q] = x2;
+        Real x1 = x2, amax = fabs(x2);
+        if (n >= 2) {
+          x1 = (Y[(n - 2) * kLdy + q] - U1[(n - 2) * kInvGroup + q] * x2) * RU0[(n - 2) * kInvGroup + q];
+          Y[(n - 2) * kLdy + q] = x1;
+          amax = fmax(amax, fabs(x1));
+        }
+        for (int i = n - 3; i >= 0; --i) {
+          const Real u2 = (SW[i * kInvGroup + q] != Real(0)) ? e[i + 1] : Real(0);
+          const Real xi = (Y[i * kLdy + q] - U1[i * kInvGroup + q] * x1 - u2 * x2) * RU0[i * kInvGroup + q];
+          Y[i * kLdy + q] = xi;
+          amax = fmax(amax, fabs(xi));
+          x2 = x1;
+          x1 = xi;
+        }
+        if (!(amax > Real(0)) || !isfinite(amax)) {
+          for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
+          continue;
+        }
+        const Real sa = Real(1) / amax;
+        Real nrm = 0;
+        for (int i = 0; i < n; ++i) {
+          const Real v = Y[i * kLdy + q] * sa;
+          Y[i * kLdy + q] = v;
+          nrm = fma(v, v, nrm);
+        }
+        const Real inv = Num<Real>::rsq(nrm);
+        for (int i = 0; i < n; ++i) Y[i * kLdy + q] *= inv;
+      }
+    }
+    __syncthreads();
+    for (int q = warp; q < g; q += 4) {
+      for (int k = n - 3; k >= 0; --k) {
+        const Real tk = tau[k];
+        if (tk == Real(0)) continue;
+        const int L = n - k - 1;
+        Real part = 0;
+        for (int i = lane; i < L; i += 32) {
+          const Real v = (i == 0) ? Real(1) : A[(k + 1 + i) * lda + k];
+          part = fma(v, Y[(k + 1 + i) * kLdy + q], part);
+        }
+        const Real f = tk * warp_sum(part);
+        for (int i = lane; i < L; i += 32) {
+          const Real v = (i == 0) ? Real(1) : A[(k + 1 + i) * lda + k];
+          Y[(k + 1 + i) * kLdy + q] = fma(-f, v, Y[(k + 1 + i) * kLdy + q]);
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int q = 0; q < g; ++q) {
+        const int j = j0 + q;
+        for (int i = 0; i < j; ++i) {
+          Real part = 0;
+          if (i < j0) {
+            for (int r = lane; r < n; r += 32) part = fma((Real)V[i * n + r], Y[r * kLdy + q], part);
+          } else {
+            for (int r = lane; r < n; r += 32) part = fma(Y[r * kLdy + (i - j0)], Y[r * kLdy + q], part);
+          }
+          const Real dot = warp_sum(part);
+          if (i < j0) {
+            for (int r = lane; r < n; r += 32) Y[r * kLdy + q] = fma(-dot, (Real)V[i * n + r], Y[r * kLdy + q]);
+          } else {
+            for (int r = lane; r < n; r += 32) Y[r * kLdy + q] = fma(-dot, Y[r * kLdy + (i - j0)], Y[r * kLdy + q]);
+          }
+          __syncwarp();
+        }
+        Real part = 0;
+        for (int r = lane; r < n; r += 32) part = fma(Y[r * kLdy + q], Y[r * kLdy + q], part);
+        const Real inv = Num<Real>::rsq(fmax(warp_sum(part), Num<Real>::tiny()));
+        for (int r = lane; r < n; r += 32) Y[r * kLdy + q] *= inv;
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < n * g; idx += NT) {
+      const int c = idx / n, r = idx - c * n;
+      V[(j0 + c) * n + r] = (float)Y[r * kLdy + c];
+    }
+  }
+  __syncthreads();
+  return margin;
+}
+
 // Shared memory bytes of eigh_refine_kernel: the float64 eigensolver's arrays
 // plus one staged z-run of the patch (pz*T floats).
 __host__ __device__ inline size_t eigh_refine_smem_bytes(int n, int pz) {
-  return sizeof(double) * eigh_smem_elems(n) + sizeof(float) * (size_t)pz * n;
+  return sizeof(double) * (eigh_smem_elems(n) + 8) + sizeof(float) * (size_t)pz * n;
 }
 
 // Float64 pass over the queued near-tie patches not yet refined:
@@ -528,7 +853,8 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
   const int n = g.nt;
   const int lda = eigh_lda(n);
   double* A = sm_ref;
-  float* run = reinterpret_cast<float*>(sm_ref + eigh_smem_elems(n));
+  double* red = sm_ref + eigh_smem_elems(n);  // block reductions (T > 64)
+  float* run = reinterpret_cast<float*>(red + 8);
   const int count = refine_count[0];
   const int first = refine_count[1];
   const int tid = threadIdx.x;
@@ -578,7 +904,10 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
       }
     }
     __syncthreads();
-    if (tid < 32)
+    if (n > 64 && nth == 128)
+      eigh_mp_block<double>(A, red, n, g.nvox_patch, vecs + pid * (long long)n * n,
+                            lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid);
+    else if (tid < 32)
       eigh_mp_warp<double>(A, n, g.nvox_patch, vecs + pid * (long long)n * n,
                            lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid);
     __syncthreads();

@@ -17,6 +17,7 @@
 #include "center.cuh"
 #include "eigh.cuh"
 #include "eigh_reg.cuh"
+#include "eigh_cta.cuh"
 #include "gram.cuh"
 #include "gram_tc.cuh"
 #include "gram_z.cuh"
@@ -117,15 +118,20 @@ namespace {
 int gramz_split(int T) { return (T > 40 && T <= 56) ? 2 : 1; }
 
 // Reconstruction thread layout for T frames: two threads per voxel up to
-// T = 96 (one shuffle per eigenvector; one thread per voxel needs ~220
-// registers at T = 48 and measured 3.4x slower), four above. The frames are
-// cut into four chunks of Q = round4(ceil(T/4)) and a thread owns 4/split
-// consecutive chunks (TPT = Q * 4 / split), so every split sums y_k in the
-// same tree.
+// T = 48, four above (a thread's frame slices, accumulators and projections
+// live in registers: 3 x T/split of them). Measured on B200, reconstruction
+// ms, brick 3x3x3, split 2 -> 4: T = 64 at 11^3 / stride 1 181 -> 82,
+// 11^3 / stride 2 27 -> 16, 5^3 / stride 1 13.5 -> 7.9; T = 96 at 7^3 /
+// stride 1 30 -> 27; T = 48 at 11^3 / stride 3 1.32 -> 1.53 (keeps 2); one
+// thread per voxel needs ~220 registers at T = 48 and measured 3.4x slower.
+// The frames are cut into four chunks of Q = round4(ceil(T/4)) and a thread
+// owns 4/split consecutive chunks (TPT = Q * 4 / split), so every split sums
+// y_k in the same tree.
 void pick_recon_layout(int T, int want_split, int& split, int& tpt) {
-  split = T <= 96 ? 2 : 4;
-  if (want_split == 1 || want_split == 2 || want_split == 4) split = std::max(want_split, split);
-  if (T > 48 && split == 1) split = 2;
+  split = T <= 48 ? 2 : 4;
+  if (want_split == 1 || want_split == 2 || want_split == 4) split = want_split;
+  if (T > 48 && split < 2) split = 2;  // one thread per voxel is built up to T = 48
+  if (T > 96 && split < 4) split = 4;  // two up to T = 96
   const int q = (((T + 3) / 4) + 3) & ~3;
   tpt = q * 4 / split;
 }
@@ -199,13 +205,15 @@ size_t eigh_smem_for(int T) {
   if (T <= 32) return lrd::eigh_reg_smem_floats<32>();
   if (T <= 48) return lrd::eigh_reg_smem_floats<48>();
   if (T <= 64) return lrd::eigh_reg_smem_floats<64>();
-  return lrd::eigh_smem_floats(T);
+  if (T <= 96) return lrd::eigh_cta_smem_floats<96>();
+  return lrd::eigh_cta_smem_floats<128>();
 }
 const void* eigh_kernel_for(int T) {
   if (T <= 32) return (const void*)lrd::eigh_reg_kernel<32>;
   if (T <= 48) return (const void*)lrd::eigh_reg_kernel<48>;
   if (T <= 64) return (const void*)lrd::eigh_reg_kernel<64>;
-  return (const void*)lrd::eigh_mp_kernel;
+  if (T <= 96) return (const void*)lrd::eigh_cta_kernel<96>;
+  return (const void*)lrd::eigh_cta_kernel<128>;
 }
 
 template <int TPT, int SPLIT>
@@ -387,9 +395,12 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
     else if (T <= 64)
       lrd::eigh_reg_kernel<64><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
                                                                         P->g.nvox_patch, p0, rcount, rids);
+    else if (T <= 96)
+      lrd::eigh_cta_kernel<96><<<(unsigned)nb, 96, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
+                                                                       P->g.nvox_patch, p0, rcount, rids);
     else
-      lrd::eigh_mp_kernel<<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
-                                                                   P->g.nvox_patch, p0, rcount, rids);
+      lrd::eigh_cta_kernel<128><<<(unsigned)nb, 128, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0,
+                                                                         T, P->g.nvox_patch, p0, rcount, rids);
     int rc = launch_check("eigh kernel launch");
     if (rc) return rc;
   }
@@ -504,6 +515,15 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     best[0] = pr->brick_x;
     best[1] = pr->brick_y;
     best[2] = pr->brick_z;
+    // the CTA must also fit the reconstruction kernel's registers
+    cudaFuncAttributes fa{};
+    for (bool acc : {false, true}) {
+      cudaError_t fe = cudaFuncGetAttributes(&fa, recon_kernel_ptr(rtpt, rsplit, acc));
+      if (fe != cudaSuccess) return cuda_fail(fe, "cudaFuncGetAttributes(recon_kernel)");
+      if ((long long)pr->brick_x * pr->brick_y * pr->brick_z * rsplit > fa.maxThreadsPerBlock)
+        return fail(LRD_ERR_INVALID, "brick %dx%dx%d x %d threads per voxel exceeds the reconstruction kernel's %d "
+                    "threads per CTA", pr->brick_x, pr->brick_y, pr->brick_z, rsplit, fa.maxThreadsPerBlock);
+    }
   }
   const int bsz[3] = {best[0], best[1], best[2]};
   for (int a = 0; a < 3; ++a) {

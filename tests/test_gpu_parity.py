@@ -209,3 +209,60 @@ def test_pipelined_host_call_equals_device_call(cuda_ok, name, form):
     dev, dr = run_dev(vol, patch, stride, form=form)
     np.testing.assert_array_equal(host, dev)
     np.testing.assert_array_equal(hr, dr)
+
+
+@pytest.mark.parametrize("shape,patch,stride", [
+    ((16, 14, 12, 96), (7, 7, 7), 2),   # one CTA per matrix, 96 threads
+    ((14, 12, 12, 128), (7, 7, 7), 2),  # 128 threads
+    ((13, 12, 11, 80), (5, 6, 5), 2),   # T between the kernels' sizes
+])
+def test_long_series_vs_live_oracle(cuda_ok, shape, patch, stride):
+    """T > 64 (block eigensolver, block float64 near-tie pass) against the
+    step-0 loop run live: ranks exact, plain within the step-0 bar, accurate
+    within the float64 bar."""
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    vol = make_phantom_lowrank(shape, seed=11)[0]
+    ref, ref_ranks = orc.denoise(vol, patch, stride)
+    out, ranks = run_dev(vol, patch, stride)
+    np.testing.assert_array_equal(ranks, ref_ranks)
+    assert rel_l2(out, ref) <= PLAIN_TOL
+    ref64, _ = orc.denoise_fp64(vol, patch, stride)
+    outa, ra = run_dev(vol, patch, stride, form="accurate")
+    np.testing.assert_array_equal(ra, ref_ranks)
+    assert rel_l2(outa, ref64) <= ACCURATE_TOL
+
+
+@pytest.mark.parametrize("T", [48, 96, 128])
+def test_stage_eigenvalues_vs_float64(cuda_ok, T):
+    """The eigensolve stage's eigenvalues of each patch's Gram matrix against
+    numpy's float64 eigvalsh of the same (device-formed) matrix."""
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    shape, patch, stride = (12, 12, 10, T), (7, 7, 5), 3
+    vol = torch.from_numpy(make_phantom_lowrank(shape, seed=2)[0]).cuda()
+    plan = api.get_plan(shape, patch, stride)
+    P = plan.n_patches
+    ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device="cuda")
+    gram = torch.empty((P, T, T), dtype=torch.float32, device="cuda")
+    vecs = torch.empty_like(gram)
+    lam = torch.empty((P, T), dtype=torch.float32, device="cuda")
+    rk = torch.empty(P, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    plan.stage_gram(vol.data_ptr(), gram.data_ptr(), ws.data_ptr(), s)
+    plan.stage_eigh(gram.data_ptr(), lam.data_ptr(), vecs.data_ptr(), rk.data_ptr(), ws.data_ptr(), s)
+    torch.cuda.synchronize()
+    g64 = gram.double().cpu().numpy()
+    ref = np.linalg.eigvalsh(g64)
+    got = lam.cpu().numpy().astype(np.float64)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert np.abs(got - ref).max() / scale.max() < 2e-6
+    # the top eigenvectors returned as rows: unit norm, G v = lambda v
+    v = vecs.cpu().numpy()
+    rks = rk.cpu().numpy()
+    for i in range(0, P, max(1, P // 8)):
+        for q in range(rks[i]):
+            x = v[i, q].astype(np.float64)
+            assert abs(np.linalg.norm(x) - 1) < 1e-5
+            lq = ref[i, T - 1 - q]
+            assert np.linalg.norm(g64[i] @ x - lq * x) <= 1e-5 * scale[i, 0]
