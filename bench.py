@@ -145,7 +145,7 @@ def run_reference(args, wl):
 
     vol, _ = make_phantom_lowrank(wl["shape"], seed=0)
     cores = host_cores()
-    per_step = args.cpu_sample or max(64, 48 * cores)
+    per_step = args.cpu_sample or max(64, 256 * cores)  # ~1 s of all cores per step
     for _ in range(args.warmup):
         cpu_step0_rate(vol, wl["patch"], wl["stride"], min(per_step, cores * 4), cores)
     rates = []
@@ -289,7 +289,7 @@ def run_ours(args, wl):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         vol0, _ = make_phantom_lowrank(shape, seed=0)
         cores = host_cores()
-        n = args.cpu_sample or max(64, 48 * cores)
+        n = args.cpu_sample or max(64, 256 * cores)  # ~10-15 s of CPU work
         rate, dt, used = cpu_step0_rate(vol0, patch, stride, n, cores)
         cpu = dict(value=rate, unit="patches/s", cores=used, kind="port",
                    sample=f"{n} patches evenly spaced over the corner list, step-0 NumPy loop "

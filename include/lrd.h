@@ -239,6 +239,18 @@ int lrd_slab_prepare(const lrd_plan* plan, const float* d_vol, int32_t* d_ranks,
 int lrd_slab_recon(const lrd_plan* plan, float* d_out, void* d_workspace, int32_t part,
                    const double* d_halo_in, double* d_halo_out, void* stream);
 
+/* Per-patch outputs of the last lrd_denoise / lrd_denoise_host /
+ * lrd_slab_prepare on ``d_workspace`` (the ladder returns only the volume,
+ * step0_numpy_loop.py:28-39; the ranks come out of every denoise call):
+ * d_sigma2 (n_patches floats, nullable) receives each patch's MP noise
+ * variance estimate, the mean of its t - p noise eigenvalues
+ * (eigs = lambda / N as in step0_numpy_loop.py:18, t = nt - 1, p the MP
+ * rank; 0 when p = t); d_noise (nx*ny*nz floats, nullable) receives the
+ * voxel noise map, the patches' estimates averaged with the denoiser's
+ * weights w = 1/(2+p) in its patch order (0 where no patch covers). Slab
+ * plans give d_sigma2 only. Enqueued on ``stream``. */
+int lrd_noise_map(const lrd_plan* plan, const void* d_workspace, float* d_sigma2, float* d_noise, void* stream);
+
 /* Message of the calling thread's last failure ("" if none). */
 const char* lrd_last_error_string(void);
 int lrd_version(void);

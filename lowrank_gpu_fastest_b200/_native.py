@@ -52,6 +52,7 @@ SIGNATURES = {
     "lrd_slab_plan_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(ctypes.c_void_p)]),
     "lrd_slab_info": (ctypes.c_int, [ctypes.c_void_p, _c_i32p]),
+    "lrd_noise_map": (ctypes.c_int, [ctypes.c_void_p] * 5),
     "lrd_slab_prepare": (ctypes.c_int, [ctypes.c_void_p] * 5),
     "lrd_slab_recon": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
@@ -181,6 +182,11 @@ class Plan:
         n = ctypes.c_int32()
         check(load().lrd_plan_phase_ms(self.handle, ms, ctypes.byref(n)))
         return dict(zip(PHASES, list(ms))), int(n.value)
+
+    def noise_map(self, d_ws, d_sigma2, d_noise, stream):
+        """Per-patch noise variance estimates and/or the voxel noise map of
+        the last denoise on ``d_ws`` (either pointer may be None)."""
+        check(load().lrd_noise_map(self.handle, d_ws, d_sigma2, d_noise, stream))
 
     def stage_gram(self, d_vol, d_gram, d_ws, stream):
         check(load().lrd_stage_gram(self.handle, d_vol, d_gram, d_ws, stream))

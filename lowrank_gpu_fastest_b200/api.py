@@ -99,6 +99,30 @@ def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", retu
     return (out, ranks) if return_ranks else out
 
 
+def denoise_with_noise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain"):
+    """``denoise`` plus the per-patch by-products of the MP step: returns a dict
+    with ``out`` (the denoised volume), ``ranks`` (per patch, x-major),
+    ``sigma2`` (per patch: the MP noise variance estimate, the mean of the
+    patch's t - p noise eigenvalues lambda / N) and ``noise`` (per voxel: the
+    covering patches' estimates averaged with the denoiser's weights 1/(2+p)).
+    numpy in -> numpy out; CUDA tensor in -> CUDA tensors (current stream)."""
+    is_np = not (torch.is_tensor(vol) and vol.is_cuda)
+    d = torch.from_numpy(np.ascontiguousarray(vol, dtype=np.float32)).cuda() if is_np else vol
+    device = d.device.index if d.device.index is not None else torch.cuda.current_device()
+    out, ranks = denoise(d, patch, stride, batch, form=form, return_ranks=True)
+    with torch.cuda.device(device):
+        plan = _plan(d.shape, patch, stride, form, batch, device)
+        stream = torch.cuda.current_stream(device)
+        ws = _workspace(plan, device, stream.cuda_stream)
+        sigma2 = torch.empty(plan.n_patches, dtype=torch.float32, device=d.device)
+        noise = torch.empty(d.shape[:3], dtype=torch.float32, device=d.device)
+        plan.noise_map(ws.data_ptr(), sigma2.data_ptr(), noise.data_ptr(), stream.cuda_stream)
+    res = dict(out=out, ranks=ranks, sigma2=sigma2, noise=noise)
+    if is_np:
+        res = {k: v.cpu().numpy() for k, v in res.items()}
+    return res
+
+
 def _denoise_host(t, patch, stride, batch, form, return_ranks, as_numpy):
     """Host -> host through ``lrd_denoise_host``: the volume moves in x-slabs
     on the plan's copy streams while earlier slabs compute; the result lands in

@@ -186,9 +186,12 @@ __device__ void bisect_all(const Real* d, const Real* e, const Real* e2, Real* l
 // MP rank from the ascending eigenvalues lam * unscale, evaluated like
 // step0_numpy_loop.py:18-24 (float32 eigs and suffix sums, float64 test,
 // a count over all indices); W holds 2n floats of scratch. Returns the
-// smallest |lhs/rhs - 1| over the indices. One warp.
+// smallest |lhs/rhs - 1| over the indices. With ``sig2_out`` lane 0 also
+// writes the patch's noise variance estimate, the mean of the t - p noise
+// eigenvalues: rcum_p / (t - p) in float32 (0 when p = t). One warp.
 template <typename Real>
-__device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float* W, int& p_out) {
+__device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float* W, int& p_out,
+                          float* sig2_out = nullptr) {
   const int lane = threadIdx.x & 31;
   // eigs = float32(max(lambda, 0) / N), as step 0's float32 s**2 / n.
   const int t = n - 1;
@@ -227,6 +230,7 @@ __device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float*
     margin = warp_min(margin);
   }
   p_out = p;
+  if (sig2_out != nullptr && lane == 0) *sig2_out = (p < t) ? __fdiv_rn(rc[p], (float)(t - p)) : 0.f;
   return margin;
 }
 
@@ -236,7 +240,7 @@ __device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float*
 // ascending eigenvalues. Returns the smallest |lhs/rhs - 1| of the MP test.
 template <typename Real>
 __device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_out, int32_t* rank_out,
-                               float* w_out) {
+                               float* w_out, float* s2_out) {
   const int lane = threadIdx.x & 31;
   const int lda = eigh_lda(n);
   Real* A = sm;                  // n x lda, symmetric working matrix
@@ -334,7 +338,7 @@ __device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_o
   Real tnorm;
   bisect_all<Real>(d, e, e2, lam, n, tnorm);
   int p;
-  const double margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p);
+  const double margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p, s2_out);
   if (lane == 0) {
     *rank_out = p;
     *w_out = (float)(1.0 / (2.0 + (double)p));
@@ -488,8 +492,8 @@ __device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_o
 // entries, order not fixed) for eigh_refine_kernel.
 __global__ void __launch_bounds__(32)
     eigh_mp_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
-                   float* __restrict__ wgt, int n, int nvox, long long patch0, int* __restrict__ refine_count,
-                   int* __restrict__ refine_ids) {
+                   float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
+                   int* __restrict__ refine_count, int* __restrict__ refine_ids) {
   extern __shared__ float sm_eig[];
   const int lane = threadIdx.x;
   const long long b = blockIdx.x;
@@ -501,7 +505,8 @@ __global__ void __launch_bounds__(32)
   }
   __syncwarp();
   const double margin = eigh_mp_warp<float>(sm_eig, n, nvox, vecs + b * (long long)n * n,
-                                            lam_out ? lam_out + b * n : nullptr, ranks + b, wgt + b);
+                                            lam_out ? lam_out + b * n : nullptr, ranks + b, wgt + b,
+                                            sig2 ? sig2 + b : nullptr);
   if (lane == 0 && refine_count != nullptr && margin < kRefineTol) {
     const int slot = atomicAdd(refine_count, 1);
     refine_ids[slot] = (int)(patch0 + b);
@@ -560,7 +565,7 @@ __device__ __forceinline__ int sturm_count1_r(const Real* d, const Real* e2, int
 
 template <typename Real>
 __device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, float* lam_out, int32_t* rank_out,
-                                float* w_out) {
+                                float* w_out, float* s2_out) {
   constexpr int NT = 128;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int lda = eigh_lda(n);
@@ -694,7 +699,7 @@ __device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, 
   double margin = 0.0;
   if (warp == 0) {
     int p;
-    margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p);
+    margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p, s2_out);
     if (lane == 0) {
       *rank_out = p;
       *w_out = (float)(1.0 / (2.0 + (double)p));
@@ -847,8 +852,9 @@ __host__ __device__ inline size_t eigh_refine_smem_bytes(int n, int pz) {
 // 0 runs the float64 eigensolver and overwrites the patch's rank, weight,
 // eigenvectors (and eigenvalues if requested).
 __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, float* __restrict__ lam_out,
-                                   int32_t* __restrict__ ranks, float* __restrict__ wgt, Geom g, AxisTables tab,
-                                   const int* __restrict__ refine_count, const int* __restrict__ refine_ids) {
+                                   int32_t* __restrict__ ranks, float* __restrict__ wgt, float* __restrict__ sig2,
+                                   Geom g, AxisTables tab, const int* __restrict__ refine_count,
+                                   const int* __restrict__ refine_ids) {
   extern __shared__ double sm_ref[];
   const int n = g.nt;
   const int lda = eigh_lda(n);
@@ -906,10 +912,12 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
     __syncthreads();
     if (n > 64 && nth == 128)
       eigh_mp_block<double>(A, red, n, g.nvox_patch, vecs + pid * (long long)n * n,
-                            lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid);
+                            lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid,
+                            sig2 ? sig2 + pid : nullptr);
     else if (tid < 32)
       eigh_mp_warp<double>(A, n, g.nvox_patch, vecs + pid * (long long)n * n,
-                           lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid);
+                           lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid,
+                           sig2 ? sig2 + pid : nullptr);
     __syncthreads();
   }
 }

@@ -93,8 +93,8 @@ __device__ __forceinline__ int sturm_count1(const float* __restrict__ d, const f
 template <int TMAX>
 __global__ void __launch_bounds__(TMAX)
     eigh_cta_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
-                    float* __restrict__ wgt, int n, int nvox, long long patch0, int* __restrict__ refine_count,
-                    int* __restrict__ refine_ids) {
+                    float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
+                    int* __restrict__ refine_count, int* __restrict__ refine_ids) {
   constexpr int NW = TMAX / 32;
   extern __shared__ __align__(16) float sc[];
   float* HV = sc;                    // TMAX x TMAX reflector vectors
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(TMAX)
   int* pshare = reinterpret_cast<int*>(red + 4 * kInvGroup + 4);
   if (warp == 0) {
     int p;
-    const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p);
+    const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p, sig2 ? sig2 + b : nullptr);
     if (lane == 0) {
       ranks[b] = p;
       wgt[b] = (float)(1.0 / (2.0 + (double)p));

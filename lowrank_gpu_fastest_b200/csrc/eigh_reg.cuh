@@ -154,8 +154,8 @@ __device__ __forceinline__ void bisect_reg(const float* d, const float* e, const
 template <int TMAX>
 __global__ void __launch_bounds__(32)
     eigh_reg_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
-                    float* __restrict__ wgt, int n, int nvox, long long patch0, int* __restrict__ refine_count,
-                    int* __restrict__ refine_ids) {
+                    float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
+                    int* __restrict__ refine_count, int* __restrict__ refine_ids) {
   constexpr int NR = eigh_reg_nr<TMAX>();
   extern __shared__ __align__(16) float sr[];
   float* HV = sr;                  // TMAX x TMAX reflector vectors
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(32)
   bisect_reg<TMAX>(d, e, e2, lam, n, tnorm);
   LRD_STAMP(3);
   int p;
-  const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p);
+  const double margin = mp_rank<float>(lam, unscale, n, nvox, W, p, sig2 ? sig2 + b : nullptr);
   if (lane == 0) {
     ranks[b] = p;
     wgt[b] = (float)(1.0 / (2.0 + (double)p));

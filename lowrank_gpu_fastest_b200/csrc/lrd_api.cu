@@ -18,6 +18,7 @@
 #include "eigh.cuh"
 #include "eigh_reg.cuh"
 #include "eigh_cta.cuh"
+#include "noise.cuh"
 #include "gram.cuh"
 #include "gram_tc.cuh"
 #include "gram_z.cuh"
@@ -78,7 +79,7 @@ struct lrd_plan {
   size_t smem_center, smem_gram, smem_eigh, smem_recon;
   int center_warps;
   // workspace offsets (bytes)
-  size_t off_mean, off_xc, off_gv, off_rank, off_wgt, off_status, off_refine, ws_bytes;
+  size_t off_mean, off_xc, off_gv, off_rank, off_wgt, off_sig2, off_status, off_refine, ws_bytes;
   size_t smem_refine;
   int refine_blocks;
   // device tables (one allocation)
@@ -380,33 +381,38 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
   const long long TT = (long long)T * T;
   int* rcount = reinterpret_cast<int*>(ws + P->off_refine);
   int* rids = rcount + 64;
+  float* sig2 = reinterpret_cast<float*>(ws + P->off_sig2);
   if (reset) LRD_CUDA(cudaMemsetAsync(rcount, 0, 2 * sizeof(int), st));
   for (long long p0 = p_lo; p0 < p_hi; p0 += batch) {
     const long long nb = std::min(batch, p_hi - p0);
     const float* gin = d_gram + p0 * TT;
     float* vout = d_vecs + p0 * TT;
     float* lout = d_lam ? d_lam + p0 * T : nullptr;
+    int32_t* r = d_rank + p0;
+    float* w = d_wgt + p0;
+    float* s2 = sig2 + p0;
+    const int nv = P->g.nvox_patch;
     if (T <= 32)
-      lrd::eigh_reg_kernel<32><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
-                                                                        P->g.nvox_patch, p0, rcount, rids);
+      lrd::eigh_reg_kernel<32><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
+                                                                        rids);
     else if (T <= 48)
-      lrd::eigh_reg_kernel<48><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
-                                                                        P->g.nvox_patch, p0, rcount, rids);
+      lrd::eigh_reg_kernel<48><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
+                                                                        rids);
     else if (T <= 64)
-      lrd::eigh_reg_kernel<64><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
-                                                                        P->g.nvox_patch, p0, rcount, rids);
+      lrd::eigh_reg_kernel<64><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
+                                                                        rids);
     else if (T <= 96)
-      lrd::eigh_cta_kernel<96><<<(unsigned)nb, 96, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0, T,
-                                                                       P->g.nvox_patch, p0, rcount, rids);
+      lrd::eigh_cta_kernel<96><<<(unsigned)nb, 96, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
+                                                                       rids);
     else
-      lrd::eigh_cta_kernel<128><<<(unsigned)nb, 128, P->smem_eigh, st>>>(gin, vout, lout, d_rank + p0, d_wgt + p0,
-                                                                         T, P->g.nvox_patch, p0, rcount, rids);
+      lrd::eigh_cta_kernel<128><<<(unsigned)nb, 128, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0,
+                                                                         rcount, rids);
     int rc = launch_check("eigh kernel launch");
     if (rc) return rc;
   }
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
-  lrd::eigh_refine_kernel<<<P->refine_blocks, 128, P->smem_refine, st>>>(xc, d_vecs, d_lam, d_rank, d_wgt, P->g,
-                                                                        P->tab, rcount, rids);
+  lrd::eigh_refine_kernel<<<P->refine_blocks, 128, P->smem_refine, st>>>(xc, d_vecs, d_lam, d_rank, d_wgt, sig2,
+                                                                        P->g, P->tab, rcount, rids);
   int rc = launch_check("eigh_refine_kernel launch");
   if (rc) return rc;
   lrd::refine_advance_kernel<<<1, 1, 0, st>>>(rcount);
@@ -669,6 +675,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   P->off_gv = off; off += align256(sizeof(float) * (size_t)g.npatch * T * T);
   P->off_rank = off; off += align256(sizeof(int32_t) * (size_t)g.npatch);
   P->off_wgt = off; off += align256(sizeof(float) * (size_t)g.npatch);
+  P->off_sig2 = off; off += align256(sizeof(float) * (size_t)g.npatch);
   P->off_status = off; off += align256(sizeof(int32_t));
   P->off_refine = off; off += align256(sizeof(int32_t) * (64 + (size_t)g.npatch));
   P->ws_bytes = off;
@@ -987,6 +994,27 @@ int lrd_slab_recon(const lrd_plan* P, float* d_out, void* d_ws, int32_t part, co
   const long long b_lo = (long long)(io.x_lo / P->g.bx) * brz;
   const long long b_hi = (long long)((io.x_hi + P->g.bx - 1) / P->g.bx) * brz;
   return run_recon(P, static_cast<char*>(d_ws), d_out, static_cast<cudaStream_t>(stream), b_lo, b_hi, &io);
+}
+
+int lrd_noise_map(const lrd_plan* P, const void* d_ws, float* d_sigma2, float* d_noise, void* stream) {
+  int rc = check_plan(P);
+  if (rc) return rc;
+  if (!d_ws) return fail(LRD_ERR_INVALID, "NULL workspace");
+  if (d_noise && P->is_slab)
+    return fail(LRD_ERR_UNSUPPORTED, "the voxel noise map of a slab needs its neighbours' patches; "
+                "take the per-patch estimates (d_sigma2) instead");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const char* ws = static_cast<const char*>(d_ws);
+  const float* sig2 = reinterpret_cast<const float*>(ws + P->off_sig2);
+  const float* wgt = reinterpret_cast<const float*>(ws + P->off_wgt);
+  if (d_sigma2)
+    LRD_CUDA(cudaMemcpyAsync(d_sigma2, sig2, sizeof(float) * P->g.npatch, cudaMemcpyDeviceToDevice, st));
+  if (d_noise) {
+    const unsigned blocks = (unsigned)((P->nvox + 255) / 256);
+    lrd::noise_map_kernel<<<blocks, 256, 0, st>>>(sig2, wgt, d_noise, P->g, P->tab);
+    return launch_check("noise_map_kernel launch");
+  }
+  return LRD_OK;
 }
 
 int lrd_workspace_status(const lrd_plan* P, const void* d_ws, int32_t* status, void* stream) {

@@ -99,6 +99,44 @@ def denoise(vol, patch=(11, 11, 11), step=3, corners=None):
     return out / np.maximum(wsum, 1e-12), ranks
 
 
+def patch_noise(x):
+    """MP rank and noise variance estimate of one ``(N, T)`` patch: the mean
+    of the t - p noise eigenvalues ``eigs = s**2 / N`` after step 0's rank
+    test (step0_numpy_loop.py:10-24): ``rcum[p] / (t - p)`` in float32, 0 when
+    p = t. The reference computes ``rcum`` but returns only the denoised
+    patch; the estimate is the package's per-patch output."""
+    n, t = x.shape
+    m = x.mean(axis=1, keepdims=True)
+    s = np.linalg.svd(x - m, compute_uv=False)[: t - 1]
+    t -= 1
+    eigs = s**2 / n
+    p = mp_rank_from_eigs(eigs, n)
+    rcum = np.cumsum(eigs[::-1])[::-1]
+    sig2 = np.float32(rcum[p] / np.float32(t - p)) if p < t else np.float32(0)
+    return p, sig2
+
+
+def noise_map(vol, patch=(11, 11, 11), step=3):
+    """Per-patch ``(ranks, sigma2)`` and the voxel map: the covering patches'
+    estimates averaged with weights 1/(2+p) in step 0's patch order and
+    float32 rounding (step0_numpy_loop.py:32-39)."""
+    vol = np.asarray(vol, dtype=np.float32)
+    px, py, pz = patch
+    corners = patch_corners(vol.shape, patch, step)
+    ranks = np.empty(len(corners), dtype=np.int32)
+    sig2 = np.empty(len(corners), dtype=np.float32)
+    acc = np.zeros(vol.shape[:3], dtype=np.float32)
+    wsum = np.zeros(vol.shape[:3], dtype=np.float32)
+    for idx, (i, j, k) in enumerate(corners):
+        x = vol[i : i + px, j : j + py, k : k + pz].reshape(-1, vol.shape[-1])
+        p, s2 = patch_noise(x)
+        ranks[idx], sig2[idx] = p, s2
+        w = np.float32(1.0 / (2.0 + p))
+        acc[i : i + px, j : j + py, k : k + pz] += w * s2
+        wsum[i : i + px, j : j + py, k : k + pz] += w
+    return ranks, sig2, acc / np.maximum(wsum, np.float32(1e-12))
+
+
 def denoise_fp64(vol, patch=(11, 11, 11), step=3):
     """FP64 oracle: the same loop on ``vol.astype(float64)``."""
     return denoise(np.asarray(vol, dtype=np.float64), patch, step)

@@ -266,3 +266,23 @@ def test_stage_eigenvalues_vs_float64(cuda_ok, T):
             assert abs(np.linalg.norm(x) - 1) < 1e-5
             lq = ref[i, T - 1 - q]
             assert np.linalg.norm(g64[i] @ x - lq * x) <= 1e-5 * scale[i, 0]
+
+
+@pytest.mark.parametrize("name", ["ref_small", "lowrank_p5s2", "lowrank_t64", "lowrank_t96", "aniso"])
+def test_noise_estimates_vs_oracle(cuda_ok, name):
+    """Per-patch MP noise variance estimates and the voxel noise map against
+    the oracle (its SVD eigenvalues differ from the Gram route's in the last
+    float32 bits, relative to the largest eigenvalue)."""
+    from lowrank_gpu_fastest_b200 import denoise_with_noise
+
+    g = load_golden(name)
+    vol = golden_input(g)
+    patch, stride = tuple(int(v) for v in g["patch"]), int(g["stride"])
+    res = denoise_with_noise(vol, patch, stride)
+    ranks, sig2, nmap = orc.noise_map(vol, patch, stride)
+    np.testing.assert_array_equal(res["ranks"], g["ranks"])
+    np.testing.assert_array_equal(res["ranks"], ranks)
+    assert np.abs(res["sigma2"] - sig2).max() <= 1e-3 * np.abs(sig2).max()
+    assert rel_l2(res["noise"], nmap) <= 1e-3
+    plain, _ = run_dev(vol, patch, stride)
+    np.testing.assert_array_equal(res["out"], plain)

@@ -93,3 +93,23 @@ def test_gram_route_stage_checker_agrees_with_svd():
     assert st["p"] == int(g["ranks64"][0])
     s = np.linalg.svd(x - x.mean(1, keepdims=True), compute_uv=False)
     np.testing.assert_allclose(np.sort(st["lam"])[::-1][:-1], s[:-1] ** 2, rtol=1e-9, atol=1e-6)
+
+
+def test_noise_map_oracle_ranks_and_scale():
+    """The noise oracle picks step 0's ranks, and on pure noise its patch
+    estimates recover the noise variance."""
+    from oracle import mppca as orc
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    vol = make_phantom_lowrank((14, 13, 12, 32), seed=0)[0]
+    ranks, sig2, nmap = orc.noise_map(vol, (5, 5, 5), 2)
+    _, ref_ranks = orc.denoise(vol, (5, 5, 5), 2)
+    np.testing.assert_array_equal(ranks, ref_ranks)
+    assert nmap.shape == vol.shape[:3] and (nmap > 0).all()
+    rng = np.random.default_rng(4)
+    noise = (rng.standard_normal((12, 12, 12, 24)) * 0.1 + 3.0).astype(np.float32)
+    r2, s2, m2 = orc.noise_map(noise, (7, 7, 7), 3)
+    assert (r2 <= 1).all() and (r2 == 0).mean() > 0.9  # the ladder's test is approximate
+    # the mean noise eigenvalue of the centred patch is sigma^2 (t-1)/t
+    assert abs(float(np.median(s2)) / (0.01 * 23 / 24) - 1) < 0.05
+    assert abs(float(m2.mean()) / (0.01 * 23 / 24) - 1) < 0.05
