@@ -9,9 +9,11 @@ headline workload is 96x96x48x48 (x, y, z, t) with 11^3 patches at stride 3
 ``value`` is whole-job patches/s from CUDA events around each step (L2 flushed
 by a 256 MiB write between steps, outside the events); ``e2e`` is the same
 metric through the C ABI's host-buffer call (pinned host in/out, both copies
-inside the timed region). Under torchrun every rank denoises its own volume
-(independent objects: weak scaling, no data-path collective); the step time is
-the max over ranks.
+inside the timed region). Under torchrun (N GPUs) the workload's volume is
+repeated N times along x and cut into N x-slabs of patch corners, one per
+rank, with one NCCL halo send/recv between neighbours per step (weak scaling:
+about the single-GPU work per rank); ``--parallel replica`` gives every rank
+an independent volume instead. The step time is the max over ranks.
 
 ``--impl reference`` times the reference algorithm's CPU implementation (the
 step-0 NumPy loop restated in oracle/, all host cores through a spawn pool)
@@ -472,6 +474,7 @@ def run_sharded(args, wl):
     def step():
         run_slab(slab, rank, world)
 
+    dist.barrier()  # brings the communicator up before the first send/recv
     for _ in range(args.warmup):
         flush.zero_()
         step()

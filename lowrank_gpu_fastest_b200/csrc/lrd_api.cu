@@ -811,6 +811,16 @@ int lrd_denoise(const lrd_plan* P, const float* d_vol, float* d_out, int32_t* d_
   return LRD_OK;
 }
 
+// End corner index of host-pipeline slab s of S over nc x-corners: the first
+// and the last slab get one corner each (the first copy-in and the last
+// copy-out are the pipeline's exposed ends), the others an equal share.
+static int slab_end(int s, int S, int nc) {
+  if (s == S - 1) return nc;
+  if (S < 4 || nc < S) return (int)((long long)(s + 1) * nc / S);
+  if (s == 0) return 1;
+  return 1 + (int)((long long)s * (nc - 2) / (S - 2));
+}
+
 int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_t* h_ranks, float* d_in,
                      float* d_out, int32_t* d_ranks, void* d_ws, void* stream) {
   int rc = check_plan(P);
@@ -850,7 +860,7 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   int planes_in = 0, ci_done = 0, bx_done = 0;
   const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
   for (int s = 0; s < S; ++s) {
-    const int ci_end = (int)((long long)(s + 1) * g.ncx / S);
+    const int ci_end = slab_end(s, S, g.ncx);
     const bool lastslab = s == S - 1;
     const int x_need = lastslab ? g.nx : std::min(g.nx, P->h_corner_x[ci_end - 1] + g.px);
     cudaStream_t prep = P->io_prep[s % 3];
