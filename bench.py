@@ -236,11 +236,12 @@ def measured_peaks():
     return dict(hbm_gbs=6650.0, bf16_tflops=1590.0, bf16_tflops_sustained=1400.0, source="of fallback")
 
 
-def fp32_simt_peak_tflops(torch):
+def fp32_simt_peak_tflops(torch, tf32=False):
     """FP32 CUDA-core GEMM throughput (cuBLAS SGEMM, TF32 off) as the FFMA
-    reference point for the float32 kernels."""
+    reference point for the float32 kernels; with ``tf32`` the same GEMM on
+    the tensor cores in TF32 (the reference point of the tensor form's Gram)."""
     old = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = bool(tf32)
     try:
         n = 8192
         a = torch.randn(n, n, device="cuda")
@@ -398,6 +399,7 @@ def run_ours(args, wl):
                         unit="GB/s", frac=achieved / peaks["hbm_gbs"], traffic=traffic,
                         peak_source=f"HBM copy {peaks['source']}")
         fp32_peak = fp32_simt_peak_tflops(torch)
+        tf32_peak = fp32_simt_peak_tflops(torch, tf32=True)
         total_flops = 4 * N * T * T * P
         line = dict(
             metric="patches_per_s", value=value, unit="patches/s", n_gpus=world, steps=args.steps,
@@ -418,7 +420,7 @@ def run_ours(args, wl):
                      path="lrd_denoise_host (pinned host in/out, H2D + denoise + D2H + sync)"),
             phases_ms=ph,
             roofline=roof,
-            fp32_simt=dict(peak_tflops_sgemm=fp32_peak,
+            fp32_simt=dict(peak_tflops_sgemm=fp32_peak, peak_tflops_tf32_gemm=tf32_peak,
                            achieved_tflops_gram_recon=total_flops / ((ph["gram"] + ph["recon"]) * 1e-3) / 1e12),
             cpu_baseline=cpu,
             clocks=clocks,

@@ -226,3 +226,52 @@ def ranks_parallel(vol, patch=(11, 11, 11), step=3, processes=None):
             else:
                 os.environ[k] = v
     return np.concatenate(parts)
+
+
+def _sums_worker(args):
+    vol, patch, corners = args
+    vol = np.asarray(vol)
+    out = np.zeros_like(vol)
+    wsum = np.zeros(vol.shape[:3] + (1,), dtype=vol.dtype)
+    px, py, pz = patch
+    ranks = np.empty(len(corners), dtype=np.int32)
+    for idx, (i, j, k) in enumerate(corners):
+        sl = np.s_[i : i + px, j : j + py, k : k + pz]
+        xd, p = mppca_patch(vol[sl].reshape(-1, vol.shape[-1]))
+        ranks[idx] = p
+        w = 1.0 / (2.0 + p)
+        out[sl] += w * xd.reshape(px, py, pz, -1)
+        wsum[sl] += w
+    return out, wsum, ranks
+
+
+def denoise_fp64_parallel(vol, patch=(11, 11, 11), step=3, processes=None):
+    """The FP64 oracle (step 0 on ``vol.astype(float64)``) over a ``spawn``
+    process pool: each worker accumulates a contiguous run of the corner
+    list, the partial sums are added in float64 (the order of those few
+    additions is the only difference from the serial loop, ~1e-16).
+    Returns ``(out, ranks)``."""
+    import multiprocessing as mp
+
+    vol = np.asarray(vol, dtype=np.float64)
+    corners = patch_corners(vol.shape, patch, step)
+    processes = processes or os.cpu_count() or 1
+    chunks = [c for c in np.array_split(corners, processes) if len(c)]
+    env_old = {k: os.environ.get(k) for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")}
+    for k in env_old:
+        os.environ[k] = "1"
+    try:
+        with mp.get_context("spawn").Pool(len(chunks)) as pool:
+            parts = pool.map(_sums_worker, [(vol, patch, c) for c in chunks])
+    finally:
+        for k, v in env_old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    out = np.zeros_like(vol)
+    wsum = np.zeros(vol.shape[:3] + (1,), dtype=np.float64)
+    for o, w, _ in parts:
+        out += o
+        wsum += w
+    return out / np.maximum(wsum, 1e-12), np.concatenate([r for _, _, r in parts])

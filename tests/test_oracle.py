@@ -113,3 +113,14 @@ def test_noise_map_oracle_ranks_and_scale():
     # the mean noise eigenvalue of the centred patch is sigma^2 (t-1)/t
     assert abs(float(np.median(s2)) / (0.01 * 23 / 24) - 1) < 0.05
     assert abs(float(m2.mean()) / (0.01 * 23 / 24) - 1) < 0.05
+
+
+def test_parallel_fp64_oracle_matches_serial():
+    from oracle import mppca as orc
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    vol = make_phantom_lowrank((12, 11, 10, 16), seed=1)[0]
+    ref, rr = orc.denoise_fp64(vol, (5, 5, 5), 2)
+    par, rp = orc.denoise_fp64_parallel(vol, (5, 5, 5), 2, processes=3)
+    np.testing.assert_array_equal(rp, rr)
+    assert np.abs(par - ref).max() <= 1e-13 * np.abs(ref).max()
