@@ -79,28 +79,40 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Shared-memory layout (bytes): hi tile (ceil(T/8) row groups of SBO bytes),
-// lo tile (same), one plane slot, windows [ring][T cols][T rows] float32,
-// mbarriers, TMEM address, abort flag. An A descriptor spans 8 row groups
-// from its tile's start (M = 64); rows past T read whatever follows (they
-// only feed accumulator rows >= T, never read), so the allocation just has to
-// cover lo + 8 groups.
+// Two-stage pipeline per column CTA (256 threads): while the tensor cores
+// run plane z's MMAs (operand tiles and TMEM accumulator of stage z & 1),
+// the CTA reads back plane z-1's Gram from the other accumulator and adds it
+// into the windows; planes arrive by TMA two ahead (two plane slots).
+//
+// Shared-memory layout (bytes): two stages of {hi tile, lo tile}
+// (ceil(T/8) row groups of SBO bytes each), two plane slots, the plane Gram
+// H (T x (T+1) floats, read back from TMEM), the windows (ring x T(T+1)/2
+// floats: upper triangle, r <= c), the upper-triangle index table
+// (T(T+1)/2 x uint32, r | c << 16), mbarriers (2 TMA + 2 MMA), TMEM address,
+// abort flag. An A descriptor spans 8 row groups from its tile's start
+// (M = 64); rows past T read whatever follows (the lo tile, or the plane
+// slots after the last tile) and only feed accumulator rows >= T, which are
+// never read back.
 __host__ __device__ inline int gramtc_kpad(int rows) { return (rows + 7) & ~7; }
 __host__ __device__ inline size_t gramtc_sbo(int rows) { return (size_t)(gramtc_kpad(rows) / 4) * 128; }
 __host__ __device__ inline size_t gramtc_tile_bytes(int rows, int T) { return (size_t)((T + 7) / 8) * gramtc_sbo(rows); }
-__host__ __device__ inline size_t gramtc_off_plane(int rows, int T) { return 2 * gramtc_tile_bytes(rows, T); }
+__host__ __device__ inline size_t gramtc_off_plane(int rows, int T) { return 4 * gramtc_tile_bytes(rows, T); }
+__host__ __device__ inline int gramtc_ntri(int T) { return T * (T + 1) / 2; }
 __host__ __device__ inline size_t gramtc_smem_bytes(int rows, int T, int ring) {
-  const size_t end = gramtc_off_plane(rows, T) +
-                     sizeof(float) * (gramz_plane_floats(rows, T) + (size_t)ring * T * T) + 64;
-  const size_t span = gramtc_tile_bytes(rows, T) + 8 * gramtc_sbo(rows);
+  const size_t planes = 2 * sizeof(float) * gramz_plane_floats(rows, T);
+  const size_t end = gramtc_off_plane(rows, T) + planes + sizeof(float) * (size_t)T * (T + 1) +
+                     sizeof(float) * (size_t)ring * gramtc_ntri(T) + sizeof(uint32_t) * gramtc_ntri(T) + 64;
+  const size_t span = 3 * gramtc_tile_bytes(rows, T) + 8 * gramtc_sbo(rows);  // stage 1's lo + 8 groups
   return end > span ? end : span;
 }
 __host__ __device__ inline int gramtc_npad(int T) { return (T + 7) & ~7; }
-__host__ __device__ inline int gramtc_tmem_cols(int T) { return gramtc_npad(T) <= 32 ? 32 : 64; }
+constexpr int kGramTcThreads = 256;
+constexpr int kIssuer = 128;  // TMA + MMA issuing thread (warp 4: no TMEM readback)
+constexpr uint32_t kGramTcCols = 128;  // two accumulators of up to 64 columns
 
-// grid: (columns in this launch); block: 128 threads (4 warps). T <= 64,
+// grid: (columns in this launch); block: kGramTcThreads. T <= 64, T % 4 == 0,
 // px*py <= 128. ``gram`` points at the Gram block of patch col0 * ncz.
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kGramTcThreads)
     gram_tc_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g, AxisTables tab,
                    long long col0, int ring, int* status) {
   extern __shared__ __align__(1024) unsigned char smt[];
@@ -109,17 +121,19 @@ __global__ void __launch_bounds__(128)
   const int kpad = gramtc_kpad(rows);
   const uint32_t sbo = (uint32_t)gramtc_sbo(rows);  // bytes between 8-row groups
   const size_t tile = gramtc_tile_bytes(rows, T);
-  unsigned char* hi = smt;
-  unsigned char* lo = smt + tile;
-  float* plane = reinterpret_cast<float*>(smt + gramtc_off_plane(rows, T));
-  float* win = plane + gramz_plane_floats(rows, T);  // [ring][T cols][T rows]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(win + (size_t)ring * T * T);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+  const size_t pf = gramz_plane_floats(rows, T);
+  const int ntri = gramtc_ntri(T);
+  const int TH = T + 1;  // H row stride (odd: conflict-free column writes)
+  float* planes = reinterpret_cast<float*>(smt + gramtc_off_plane(rows, T));  // two slots of pf floats
+  float* H = planes + 2 * pf;
+  float* win = H + (size_t)T * TH;  // [ring][ntri]
+  uint32_t* tri = reinterpret_cast<uint32_t*>(win + (size_t)ring * ntri);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tri + ntri + ((ntri & 1) ? 1 : 0));  // 8-byte aligned
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);  // set when a wait gave up
-  const uint32_t bart = (uint32_t)__cvta_generic_to_shared(&bars[0]);
-  const uint32_t barm = (uint32_t)__cvta_generic_to_shared(&bars[1]);
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
+  const int nth = blockDim.x;
 
   const long long col = col0 + blockIdx.x;
   const int ci = (int)(col / g.ncy), cj = (int)(col % g.ncy);
@@ -127,22 +141,25 @@ __global__ void __launch_bounds__(128)
   const uint32_t plane_bytes = (uint32_t)(rows * T * sizeof(float));
   const int Npad = gramtc_npad(T);
   const uint32_t idesc = umma_idesc_tf32(64, Npad);
-  const uint32_t ncols = (uint32_t)gramtc_tmem_cols(T);
   const int nv4 = (rows + 3) >> 2;
 
-  // zero the operand tiles once (rows >= T and voxels >= rows stay zero) and the windows
-  for (size_t e = tid; e < 2 * tile / 16; e += blockDim.x) reinterpret_cast<uint4*>(smt)[e] = make_uint4(0, 0, 0, 0);
-  for (int e = tid; e < ring * T * T; e += blockDim.x) win[e] = 0.f;
+  // zero both stages' operand tiles (rows >= T and voxels >= rows stay zero) and the windows;
+  // the upper-triangle table
+  for (size_t e = tid; e < 4 * tile / 16; e += nth) reinterpret_cast<uint4*>(smt)[e] = make_uint4(0, 0, 0, 0);
+  for (int e = tid; e < ring * ntri; e += nth) win[e] = 0.f;
+  for (int r = warp; r < T; r += nth / 32) {
+    const int base = r * T - r * (r - 1) / 2;  // index of (r, r)
+    for (int c = r + lane; c < T; c += 32) tri[base + (c - r)] = (uint32_t)r | ((uint32_t)c << 16);
+  }
   if (tid == 0) {
     *abort_flag = 0;
-    mbar_init(bart, 1);
-    mbar_init(barm, 1);
+    for (int i = 0; i < 4; ++i) mbar_init((uint32_t)__cvta_generic_to_shared(&bars[i]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      (uint32_t)__cvta_generic_to_shared(tmem_slot)),
-                 "r"(ncols)
+                 "r"(kGramTcCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -150,99 +167,123 @@ __global__ void __launch_bounds__(128)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t hi_addr = (uint32_t)__cvta_generic_to_shared(hi);
-  const uint32_t lo_addr = (uint32_t)__cvta_generic_to_shared(lo);
-  const uint32_t plane_addr = (uint32_t)__cvta_generic_to_shared(plane);
+  const uint32_t smt_addr = (uint32_t)__cvta_generic_to_shared(smt);
+  const uint32_t planes_addr = (uint32_t)__cvta_generic_to_shared(planes);
+  auto bar_tma = [&](int s) { return (uint32_t)__cvta_generic_to_shared(&bars[s]); };
+  auto bar_mma = [&](int s) { return (uint32_t)__cvta_generic_to_shared(&bars[2 + s]); };
 
-  if (tid == 0 && g.nz > 0) {
-    mbar_expect_tx(bart, plane_bytes);
-    tma_load_4d(plane_addr, &xmap, bart, 0, 0, cy, cx);
+  if (tid == kIssuer) {
+    for (int z = 0; z < 2 && z < g.nz; ++z) {
+      mbar_expect_tx(bar_tma(z), plane_bytes);
+      tma_load_4d(planes_addr + (uint32_t)(z * pf * sizeof(float)), &xmap, bar_tma(z), 0, z, cy, cx);
+    }
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
-  uint32_t mma_phase = 0;
-  // the row of H (and of the windows) this thread owns: t = 16*warp + lane, lanes 0..15
-  const int trow = warp * 16 + lane;
-  const bool owner = lane < 16 && trow < T;
-  for (int z = 0; z < g.nz; ++z) {
-    if (*abort_flag) break;  // uniform: read after the barrier closing the previous plane
-    if (!mbar_wait_bounded(bart, (uint32_t)(z & 1), status)) *abort_flag = 1;
-    const int klo = tab.cover[2][2 * z], khi = tab.cover[2][2 * z + 1];
-    const bool active = klo <= khi;  // uniform
-    if (active) {
-      // split into the hi / lo K-major tiles; item (t, 4 voxels) -> one 16-byte
-      // core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16
-      for (int e = tid; e < T * nv4; e += blockDim.x) {
-        const int v4 = e / T, t = e - v4 * T;
-        uint32_t h[4], l[4];
+
+  // Reads back plane zr's Gram (accumulator zr & 1) into H and adds it into
+  // the windows it belongs to; writes out the windows it completes.
+  auto drain = [&](int zr) {
+    const int s = zr & 1;
+    if (!mbar_wait_bounded(bar_mma(s), (uint32_t)((zr >> 1) & 1), status, kStatusMmaTimeout)) *abort_flag = 1;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (warp < 4 && warp * 16 < T) {  // M = 64: rows 16w..16w+15 in lanes 0..15 of sub-partition w
+      const int trow = warp * 16 + lane;
+      for (int c0 = 0; c0 < Npad; c0 += 16) {
+        float h[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * 64 + c0), h);
+        if (lane < 16 && trow < T) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int v = 4 * v4 + i;
-          const float x = v < rows ? plane[v * T + t] : 0.f;
-          h[i] = tf32_rna(x);
-          l[i] = tf32_rna(x - __uint_as_float(h[i]));
+          for (int c = 0; c < 16; ++c)
+            if (c0 + c < T) H[trow * TH + c0 + c] = h[c];
         }
-        const uint32_t off = (uint32_t)(t >> 3) * sbo + (uint32_t)v4 * 128 + (uint32_t)(t & 7) * 16;
-        *reinterpret_cast<uint4*>(hi + off) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(lo + off) = make_uint4(l[0], l[1], l[2], l[3]);
       }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();  // H complete; the accumulator is free for plane zr + 2
+    const int klo = tab.cover[2][2 * zr], khi = tab.cover[2][2 * zr + 1];
+    bool done_any = false;
+    for (int e = tid; e < ntri; e += nth) {
+      const uint32_t rc = tri[e];
+      const float h = H[(rc & 0xffff) * TH + (rc >> 16)];
+      for (int k = klo; k <= khi; ++k) win[(size_t)(k % ring) * ntri + e] += h;
+    }
+    for (int k = klo; k <= khi; ++k) done_any |= zr == tab.corners[2][k] + g.pz - 1;
+    if (done_any) {  // uniform
+      __syncthreads();
+      for (int k = klo; k <= khi; ++k) {
+        if (zr != tab.corners[2][k] + g.pz - 1) continue;
+        const float* w = win + (size_t)(k % ring) * ntri;
+        float* G = G0 + (size_t)k * T * T;
+        for (int r = warp; r < T; r += nth / 32)
+          for (int c = lane; c < T; c += 32) {
+            const int a = min(r, c), b2 = max(r, c);
+            G[r * T + c] = w[a * T - a * (a - 1) / 2 + (b2 - a)];
+          }
+      }
+      __syncthreads();
+      for (int k = klo; k <= khi; ++k) {
+        if (zr != tab.corners[2][k] + g.pz - 1) continue;
+        float* w = win + (size_t)(k % ring) * ntri;
+        for (int e = tid; e < ntri; e += nth) w[e] = 0.f;
+      }
+    }
+    __syncthreads();  // H and the windows are rewritten by the next drain
+  };
+
+  for (int z = 0; z < g.nz; ++z) {
+    if (*abort_flag) break;  // uniform: read after the barrier closing the previous step
+    const int s = z & 1;
+    if (!mbar_wait_bounded(bar_tma(s), (uint32_t)((z >> 1) & 1), status)) *abort_flag = 1;
+    // split plane z into stage s's hi / lo K-major tiles; item (t, 4 voxels) ->
+    // one 16-byte core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16. Stage s
+    // was last read by plane z-2's MMAs, drained in step z-1.
+    const float* pl = planes + (size_t)s * pf;
+    unsigned char* hi = smt + (size_t)s * 2 * tile;
+    unsigned char* lo = hi + tile;
+    for (int e = tid; e < T * nv4; e += nth) {
+      const int v4 = e / T, t = e - v4 * T;
+      uint32_t hh[4], ll[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int v = 4 * v4 + i;
+        const float x = v < rows ? pl[v * T + t] : 0.f;
+        hh[i] = tf32_rna(x);
+        ll[i] = tf32_rna(x - __uint_as_float(hh[i]));
+      }
+      const uint32_t off = (uint32_t)(t >> 3) * sbo + (uint32_t)v4 * 128 + (uint32_t)(t & 7) * 16;
+      *reinterpret_cast<uint4*>(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+      *reinterpret_cast<uint4*>(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();  // tiles written, plane slot free
-    if (tid == 0) {
-      if (z + 1 < g.nz) {  // next plane streams in while this one's MMAs run
-        mbar_expect_tx(bart, plane_bytes);
-        tma_load_4d(plane_addr, &xmap, bart, 0, z + 1, cy, cx);
+    __syncthreads();  // tiles written, plane slot s free
+    if (tid == kIssuer) {  // a thread of a warp that does not read TMEM back
+      if (z + 2 < g.nz) {
+        mbar_expect_tx(bar_tma(s), plane_bytes);
+        tma_load_4d(planes_addr + (uint32_t)(s * pf * sizeof(float)), &xmap, bar_tma(s), 0, z + 2, cy, cx);
       }
-      if (active) {
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        uint32_t acc = 0;
-        for (int ks = 0; ks < kpad / 8; ++ks) {
-          const uint32_t koff = (uint32_t)ks * 256;  // 8 tf32 = two core matrices along K
-          const uint64_t dh = umma_desc_kmajor(hi_addr + koff, 128, sbo);
-          const uint64_t dl = umma_desc_kmajor(lo_addr + koff, 128, sbo);
-          umma_tf32(tmem, dh, dh, idesc, acc);
-          umma_tf32(tmem, dh, dl, idesc, 1);
-          umma_tf32(tmem, dl, dh, idesc, 1);
-          acc = 1;
-        }
-        umma_commit(barm);
-      }
-    }
-    if (active) {
-      if (!mbar_wait_bounded(barm, mma_phase, status, kStatusMmaTimeout)) *abort_flag = 1;
-      mma_phase ^= 1;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      if (warp * 16 < T) {
-        for (int c0 = 0; c0 < Npad; c0 += 16) {
-          float h[16];
-          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, h);
-          if (owner) {
-            for (int k = klo; k <= khi; ++k) {
-              float* w = win + (size_t)(k % ring) * T * T + trow;  // column c at w[c * T]
-              const bool last = z == tab.corners[2][k] + g.pz - 1;
-              float* G = G0 + (size_t)k * T * T + (size_t)trow * T;
-#pragma unroll
-              for (int c = 0; c < 16; ++c) {
-                if (c0 + c < T) {
-                  const float val = w[(size_t)(c0 + c) * T] + h[c];
-                  if (last) {
-                    G[c0 + c] = val;
-                    w[(size_t)(c0 + c) * T] = 0.f;
-                  } else {
-                    w[(size_t)(c0 + c) * T] = val;
-                  }
-                }
-              }
-            }
-          }
-        }
+      const uint32_t hi_addr = smt_addr + (uint32_t)(s * 2 * tile), lo_addr = hi_addr + (uint32_t)tile;
+      const uint32_t acc_addr = tmem + (uint32_t)(s * 64);
+      // the descriptors' start-address field is address >> 4: one K step (8 tf32
+      // = two 128-byte core matrices) adds 16 to it
+      uint64_t dh = umma_desc_kmajor(hi_addr, 128, sbo), dl = umma_desc_kmajor(lo_addr, 128, sbo);
+      uint32_t acc = 0;
+      for (int ks = 0; ks < kpad / 8; ++ks) {
+        umma_tf32(acc_addr, dh, dh, idesc, acc);
+        umma_tf32(acc_addr, dh, dl, idesc, 1);
+        umma_tf32(acc_addr, dl, dh, idesc, 1);
+        acc = 1;
+        dh += 16;
+        dl += 16;
       }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      umma_commit(bar_mma(s));
     }
-    __syncthreads();  // TMEM and tiles rewritten next plane
+    if (z >= 1) drain(z - 1);  // overlaps plane z's MMAs
+    else __syncthreads();
   }
+  if (!*abort_flag && g.nz > 0) drain(g.nz - 1);
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(ncols) : "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kGramTcCols) : "memory");
 }
 
 }  // namespace lrd

@@ -344,7 +344,7 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
     for (long long c0 = col_lo; c0 < col_hi; c0 += cols) {
       const long long nc = std::min(cols, col_hi - c0);
       if (P->use_gramtc) {
-        lrd::gram_tc_kernel<<<(unsigned)nc, 128, P->smem_gramtc, st>>>(map, d_gram + c0 * P->g.ncz * TT, P->g,
+        lrd::gram_tc_kernel<<<(unsigned)nc, lrd::kGramTcThreads, P->smem_gramtc, st>>>(map, d_gram + c0 * P->g.ncz * TT, P->g,
                                                                       P->tab, c0, P->gramz_ring, status);
         rc = launch_check("gram_tc_kernel launch");
       } else {
