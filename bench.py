@@ -376,28 +376,11 @@ def run_ours(args, wl):
     e2e_ms_step = float(t.item())
 
     if rank == 0:
-        vbytes = int(np.prod(shape)) * 4
-        peaks = measured_peaks()
         ph = {k: v / max(ncalls, 1) for k, v in phases.items()}
-        dom = max(ph, key=ph.get)
+        roof = roofline(ph, shape, patch, P, args.form)
         N = int(np.prod(patch))
         T = shape[3]
-        flops_unit = {"gram": 2 * N * T * T, "recon": 2 * N * T * T}
-        kname = phase_kernel(dom, T, args.form)
-        traffic = ncu_traffic().get(kname)
-        if dom in flops_unit:
-            achieved = flops_unit[dom] * P / (ph[dom] * 1e-3) / 1e12
-            roof = dict(kernel=kname, bound="tensor", achieved=achieved,
-                        peak=peaks["bf16_tflops"], unit="TFLOP/s",
-                        frac=achieved / peaks["bf16_tflops"], traffic=traffic,
-                        peak_source=f"bf16 dense burst {peaks['source']}",
-                        algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch")
-        else:
-            byts = {"center": 2 * vbytes + vbytes // T, "eigh_mp": 2 * P * T * T * 4}[dom]
-            achieved = byts / (ph[dom] * 1e-3) / 1e9
-            roof = dict(kernel=kname, bound="hbm", achieved=achieved, peak=peaks["hbm_gbs"],
-                        unit="GB/s", frac=achieved / peaks["hbm_gbs"], traffic=traffic,
-                        peak_source=f"HBM copy {peaks['source']}")
+        vbytes = int(np.prod(shape)) * 4
         fp32_peak = fp32_simt_peak_tflops(torch)
         tf32_peak = fp32_simt_peak_tflops(torch, tf32=True)
         total_flops = 4 * N * T * T * P
@@ -433,6 +416,36 @@ def run_ours(args, wl):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def roofline(ph, shape, patch, P, form):
+    """``roofline`` object for the dominant phase of one denoise (phase ms
+    ``ph``): algorithmic FLOPs (Gram, reconstruction: 2 N T^2 per patch) or
+    bytes (centre: volume in/out + means; eigensolve: Gram block in and
+    eigenvector block out, 2 T^2 x 4 per patch) per launch over the phase's
+    event time, against the measured peaks; DRAM traffic per launch from the
+    committed ncu summary."""
+    peaks = measured_peaks()
+    dom = max(ph, key=ph.get)
+    N = int(np.prod(patch))
+    T = shape[3]
+    vbytes = int(np.prod(shape)) * 4
+    flops_unit = {"gram": 2 * N * T * T, "recon": 2 * N * T * T}
+    kname = phase_kernel(dom, T, form)
+    traffic = ncu_traffic().get(kname)
+    if dom in flops_unit:
+        achieved = flops_unit[dom] * P / (ph[dom] * 1e-3) / 1e12
+        return dict(kernel=kname, bound="tensor", achieved=achieved, peak=peaks["bf16_tflops"], unit="TFLOP/s",
+                    frac=achieved / peaks["bf16_tflops"], traffic=traffic,
+                    peak_source=f"bf16 dense burst {peaks['source']}",
+                    algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch")
+    byts = {"center": 2 * vbytes + vbytes // T, "eigh_mp": 2 * P * T * T * 4}[dom]
+    achieved = byts / (ph[dom] * 1e-3) / 1e9
+    return dict(kernel=kname, bound="hbm", achieved=achieved, peak=peaks["hbm_gbs"], unit="GB/s",
+                frac=achieved / peaks["hbm_gbs"], traffic=traffic, peak_source=f"HBM copy {peaks['source']}",
+                algorithmic=f"{byts / P:.0f} B/patch x {P} patches per launch",
+                note="the eigensolver is latency-bound (Householder and Sturm recurrences), not HBM-bound"
+                if dom == "eigh_mp" else None)
 
 
 def run_sharded(args, wl):
@@ -522,6 +535,24 @@ def run_sharded(args, wl):
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_ms_step = float(t.item())
     halo_bytes = slab.halo_out.numel() * 8
+    roof = None
+    if rank == 0:  # the per-GPU kernels' roofline: phase events of the single-GPU workload's plan
+        from lowrank_gpu_fastest_b200 import api
+
+        plan = api.get_plan(wl["shape"], patch, stride, form=args.form, device=local)
+        d_vol = torch.from_numpy(base).to(dev)
+        d_out = torch.empty_like(d_vol)
+        ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=dev)
+        for _ in range(2):
+            plan.denoise(d_vol.data_ptr(), d_out.data_ptr(), None, ws.data_ptr(), stream.cuda_stream)
+        plan.set_profiling(True)
+        for _ in range(3):
+            plan.denoise(d_vol.data_ptr(), d_out.data_ptr(), None, ws.data_ptr(), stream.cuda_stream)
+        phases, ncalls = plan.phase_ms()
+        plan.set_profiling(False)
+        roof = roofline({k: v / max(ncalls, 1) for k, v in phases.items()}, wl["shape"], patch,
+                        plan.n_patches, args.form)
+        del d_vol, d_out, ws
     if rank == 0:
         line = dict(
             metric="patches_per_s", value=value, unit="patches/s", n_gpus=world, steps=args.steps,
@@ -539,6 +570,8 @@ def run_sharded(args, wl):
                      path="per rank: H2D of its slab planes, slab step with halo exchange, D2H of owned "
                           "planes (rank 0's bytes; max time over ranks)"),
             clocks=clocks,
+            roofline=roof,
+            cpu_baseline=None,
             gpu_launches=launches * args.steps,
             gpu_launches_note="rank 0's own kernels (NCCL's send/recv kernels not counted)",
         )
