@@ -49,7 +49,7 @@ def phase_kernel(phase, T, form):
     if phase == "gram":
         return "gram_tc_kernel" if (form == "tensor" and T <= 64) else "gram_z_kernel"
     if phase == "eigh_mp":
-        return "eigh_reg_kernel" if T <= 64 else "eigh_mp_kernel"
+        return "eigh_reg_kernel" if T <= 64 else "eigh_cta_kernel"
     return {"center": "center_kernel", "recon": "recon_kernel"}[phase]
 
 

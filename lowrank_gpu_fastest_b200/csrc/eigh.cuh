@@ -104,7 +104,6 @@ __host__ __device__ inline int eigh_lda(int n) { return n + ((n & 1) ? 2 : 1); }
 __host__ __device__ inline size_t eigh_smem_elems(int n) {
   return (size_t)n * eigh_lda(n) + (size_t)n * kLdy + 5 * (size_t)n + (size_t)4 * n * kInvGroup;
 }
-__host__ __device__ inline size_t eigh_smem_floats(int n) { return eigh_smem_elems(n); }
 
 // Sturm counts of two shifts at once (two independent dependency chains per lane).
 template <typename Real>
@@ -483,34 +482,6 @@ __device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_o
     __syncwarp();
   }
   return margin;
-}
-
-// Main pass: one warp per patch, float32. grid: one block of 32 threads per
-// patch of this launch (patch index patch0 + blockIdx.x). ``gram`` (read) and
-// ``vecs`` (written) may alias: the block reads its whole matrix before
-// writing. Near-tie patches are appended to ``refine_ids`` (``refine_count``
-// entries, order not fixed) for eigh_refine_kernel.
-__global__ void __launch_bounds__(32)
-    eigh_mp_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
-                   float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
-                   int* __restrict__ refine_count, int* __restrict__ refine_ids) {
-  extern __shared__ float sm_eig[];
-  const int lane = threadIdx.x;
-  const long long b = blockIdx.x;
-  const int lda = eigh_lda(n);
-  const float* G = gram + b * (long long)n * n;
-  for (int idx = lane; idx < n * n; idx += 32) {
-    const int r = idx / n, c = idx - r * n;
-    sm_eig[r * lda + c] = G[idx];
-  }
-  __syncwarp();
-  const double margin = eigh_mp_warp<float>(sm_eig, n, nvox, vecs + b * (long long)n * n,
-                                            lam_out ? lam_out + b * n : nullptr, ranks + b, wgt + b,
-                                            sig2 ? sig2 + b : nullptr);
-  if (lane == 0 && refine_count != nullptr && margin < kRefineTol) {
-    const int slot = atomicAdd(refine_count, 1);
-    refine_ids[slot] = (int)(patch0 + b);
-  }
 }
 
 // One CTA of 128 threads: the same decomposition as eigh_mp_warp<Real> for

@@ -200,10 +200,14 @@ __global__ void __launch_bounds__(32)
     if (lane == (k & 31)) {
       if (NR == 1 || k < 32) {
 #pragma unroll
-        for (int j = 0; j < TMAX; ++j) xk[j] = a[0][j];
+        for (int j4 = 0; j4 < TMAX / 4; ++j4)
+          reinterpret_cast<float4*>(xk)[j4] = make_float4(a[0][4 * j4], a[0][4 * j4 + 1], a[0][4 * j4 + 2],
+                                                          a[0][4 * j4 + 3]);
       } else {
 #pragma unroll
-        for (int j = 0; j < TMAX; ++j) xk[j] = a[NR - 1][j];
+        for (int j4 = 0; j4 < TMAX / 4; ++j4)
+          reinterpret_cast<float4*>(xk)[j4] = make_float4(a[NR - 1][4 * j4], a[NR - 1][4 * j4 + 1],
+                                                          a[NR - 1][4 * j4 + 2], a[NR - 1][4 * j4 + 3]);
       }
     }
     __syncwarp();
