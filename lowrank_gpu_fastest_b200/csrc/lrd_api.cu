@@ -856,7 +856,10 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   LRD_CUDA(cudaStreamWaitEvent(P->io_out, start, 0));
   for (auto ps : P->io_prep) LRD_CUDA(cudaStreamWaitEvent(ps, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
-  const int S = std::max(1, std::min(kIoSlabsUsed, g.ncx));
+  // about 8 MiB of input per slab, at most kIoSlabsUsed slabs: a small volume's
+  // slabs would be launch- and event-bound
+  const long long vbytes = (long long)sizeof(float) * P->nvox * g.nt;
+  const int S = std::max(1, std::min<int>({kIoSlabsUsed, g.ncx, (int)((vbytes + (8ll << 20) - 1) >> 23)}));
   int planes_in = 0, ci_done = 0, bx_done = 0;
   const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
   for (int s = 0; s < S; ++s) {
