@@ -125,11 +125,14 @@ int gramz_split(int T) { return (T > 40 && T <= 56) ? 2 : 1; }
 // 11^3 / stride 2 27 -> 16, 5^3 / stride 1 13.5 -> 7.9; T = 96 at 7^3 /
 // stride 1 30 -> 27; T = 48 at 11^3 / stride 3 1.32 -> 1.53 (keeps 2); one
 // thread per voxel needs ~220 registers at T = 48 and measured 3.4x slower.
+// The forms that accumulate in float64 (accurate, tensor) take four threads
+// at every T: their accumulators double the registers (T = 48 headline:
+// 3.62 -> 1.68 ms).
 // The frames are cut into four chunks of Q = round4(ceil(T/4)) and a thread
 // owns 4/split consecutive chunks (TPT = Q * 4 / split), so every split sums
 // y_k in the same tree.
-void pick_recon_layout(int T, int want_split, int& split, int& tpt) {
-  split = T <= 48 ? 2 : 4;
+void pick_recon_layout(int T, int want_split, bool acc64, int& split, int& tpt) {
+  split = (T <= 48 && !acc64) ? 2 : 4;
   if (want_split == 1 || want_split == 2 || want_split == 4) split = want_split;
   if (T > 48 && split < 2) split = 2;  // one thread per voxel is built up to T = 48
   if (T > 96 && split < 4) split = 4;  // two up to T = 96
@@ -511,7 +514,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   int rsplit = 1, rtpt = 4;
   if (pr->recon_split != 0 && pr->recon_split != 1 && pr->recon_split != 2 && pr->recon_split != 4)
     return fail(LRD_ERR_INVALID, "recon_split must be 0, 1, 2 or 4, got %d", pr->recon_split);
-  pick_recon_layout(pr->nt, pr->recon_split, rsplit, rtpt);
+  pick_recon_layout(pr->nt, pr->recon_split, pr->form != LRD_FORM_PLAIN, rsplit, rtpt);
   choose_brick(dims, pat, corners, rsplit, best);
   if (pr->brick_x > 0 || pr->brick_y > 0 || pr->brick_z > 0) {
     if (pr->brick_x < 1 || pr->brick_y < 1 || pr->brick_z < 1 ||

@@ -286,3 +286,14 @@ def test_noise_estimates_vs_oracle(cuda_ok, name):
     assert rel_l2(res["noise"], nmap) <= 1e-3
     plain, _ = run_dev(vol, patch, stride)
     np.testing.assert_array_equal(res["out"], plain)
+
+
+def test_host_pipeline_with_patch_batches(cuda_ok):
+    """The ladder's BATCH (patches per Gram / eigensolver launch) through the
+    pipelined host call equals the device call without batching."""
+    g = load_golden("lowrank_p5s2")
+    vol = golden_input(g)
+    host, hr = api.denoise(vol, (5, 5, 5), 2, batch=23, return_ranks=True)
+    dev, dr = run_dev(vol, (5, 5, 5), 2)
+    np.testing.assert_array_equal(hr, dr)
+    np.testing.assert_array_equal(host, dev)
