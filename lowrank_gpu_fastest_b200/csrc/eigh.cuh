@@ -637,7 +637,11 @@ __device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, 
   for (int i = tid; i < n; i += NT) e2[i] = (i < n - 1) ? e[i] * e[i] : Real(0);
   __syncthreads();
 
-  // bisection, thread j = eigenvalue j (bisect_all's interval rule and stopping test)
+  // bisection, thread j = eigenvalue j, after a multisection pass (counts at
+  // 128 evenly spaced points of the Gerschgorin interval bracket every
+  // eigenvalue at once). The float64 pass exists to settle the MP test and the
+  // top eigenvectors, so it stops at 100 eps (1e-14 relative to the norm
+  // bound, and to the eigenvalue): ~40 steps instead of ~57.
   Real tnorm;
   {
     Real glo = Num<Real>::huge(), ghi = -Num<Real>::huge();
@@ -652,11 +656,22 @@ __device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, 
     glo -= Real(4) * eps * tnorm * n;
     ghi += Real(4) * eps * tnorm * n;
     const Real pivmin = Num<Real>::tiny() * Real(4);
-    const Real abstol = Real(0.1) * eps * tnorm;
+    const Real loose = Real(100) * eps;
+    const Real abstol = loose * tnorm;
+    const Real h = (ghi - glo) / Real(NT + 1);
+    int* cnt = reinterpret_cast<int*>(W);
+    cnt[tid] = sturm_count1_r(d, e2, n, glo + Real(tid + 1) * h, pivmin);
+    __syncthreads();
     for (int j = tid; j < n; j += NT) {
-      Real lo = glo, hi = ghi;
+      int lo_m = -1, hi_m = NT;  // cnt[lo_m] <= j < cnt[hi_m] holds along the search
+      while (hi_m - lo_m > 1) {
+        const int mid = (lo_m + hi_m) >> 1;
+        if (cnt[mid] <= j) lo_m = mid; else hi_m = mid;
+      }
+      Real lo = lo_m >= 0 ? glo + Real(lo_m + 1) * h : glo;
+      Real hi = hi_m < NT ? glo + Real(hi_m + 1) * h : ghi;
       for (int it = 0; it < 200; ++it) {
-        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo), fabs(hi)));
+        const Real tol = fmax(abstol, Real(2) * loose * fmax(fabs(lo), fabs(hi)));
         const Real mid = Real(0.5) * (lo + hi);
         if (!(hi - lo > tol && mid > lo && mid < hi)) break;
         if (sturm_count1_r(d, e2, n, mid, pivmin) > j) hi = mid; else lo = mid;
