@@ -825,18 +825,25 @@ __device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, 
 }
 
 // Shared memory bytes of eigh_refine_kernel: the float64 eigensolver's arrays
-// plus one staged z-run of the patch (pz*T floats).
+// plus two staged z-runs of the patch (pz*T floats each).
 __host__ __device__ inline size_t eigh_refine_smem_bytes(int n, int pz) {
-  return sizeof(double) * (eigh_smem_elems(n) + 8) + sizeof(float) * (size_t)pz * n;
+  return sizeof(double) * (eigh_smem_elems(n) + 8) + 2 * sizeof(float) * (size_t)pz * n;
 }
+
+constexpr int kRefineEntries = 24;  // Gram entries per thread per pass over the patch
+constexpr int kRefinePrefetch = 16; // floats of the next z-run a thread prefetches
 
 // Float64 pass over the queued near-tie patches not yet refined:
 // refine_count[0] = entries queued, refine_count[1] = entries already refined
 // (advanced by refine_advance_kernel after this kernel). Persistent grid, one
-// patch per block at a time. The block forms G = Xc^T Xc in float64 (products of the
-// float32 centred values are exact in float64, the sum is float64), then warp
-// 0 runs the float64 eigensolver and overwrites the patch's rank, weight,
-// eigenvectors (and eigenvalues if requested).
+// patch per block at a time (128 threads). The block forms G = Xc^T Xc in
+// float64 (products of the float32 centred values are exact in float64, the
+// sum is float64) in passes of kRefineEntries entries per thread over the
+// patch's z-runs, the next run prefetched through registers into a second
+// buffer; then the block's float64 eigensolver (eigh_mp_block) overwrites the
+// patch's rank, weight, eigenvectors (and eigenvalues if requested). A queue
+// holds a handful of patches per volume, so this pass is one patch's latency:
+// every step of it is spread over the block.
 __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, float* __restrict__ lam_out,
                                    int32_t* __restrict__ ranks, float* __restrict__ wgt, float* __restrict__ sig2,
                                    Geom g, AxisTables tab, const int* __restrict__ refine_count,
@@ -845,65 +852,96 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
   const int n = g.nt;
   const int lda = eigh_lda(n);
   double* A = sm_ref;
-  double* red = sm_ref + eigh_smem_elems(n);  // block reductions (T > 64)
-  float* run = reinterpret_cast<float*>(red + 8);
+  double* red = sm_ref + eigh_smem_elems(n);  // block reductions
+  float* runs = reinterpret_cast<float*>(red + 8);  // two z-run buffers
+  const int runlen = g.pz * n;
   const int count = refine_count[0];
   const int first = refine_count[1];
   const int tid = threadIdx.x;
   const int nth = blockDim.x;
   const int nent = n * (n + 1) / 2;
+  const int nruns = g.px * g.py;
+  // the next run goes through registers while this one is used (one barrier
+  // per run) when a thread's share fits kRefinePrefetch floats
+  const bool prefetch = runlen <= kRefinePrefetch * nth;
   for (int w = first + blockIdx.x; w < count; w += gridDim.x) {
     const long long pid = refine_ids[w];
     int ci, cj, ck;
     patch_axes(g, pid, ci, cj, ck);
     const int cx = tab.corners[0][ci], cy = tab.corners[1][cj], cz = tab.corners[2][ck];
-    for (int base = 0; base < nent; base += 8 * nth) {
-      int ei[8], ej[8];
-      bool live[8];
-      double acc[8];
+    auto run_src = [&](int q) { return xc + voxel_row(g, cx + q / g.py, cy + q % g.py, cz) * n; };
+    // G = Xc^T Xc in float64 (products of float32 values are exact in float64);
+    // entry (r, c), r <= c, sums over the runs in x-major voxel order
+    for (int base = 0; base < nent; base += kRefineEntries * nth) {
+      uint32_t rc[kRefineEntries];
+      double acc[kRefineEntries];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < kRefineEntries; ++u) {
         int e = base + tid + u * nth, r = 0;
-        live[u] = e < nent;
-        if (live[u])
+        if (e < nent) {
           while (e >= n - r) {
             e -= n - r;
             ++r;
           }
-        ei[u] = live[u] ? r : 0;
-        ej[u] = live[u] ? r + e : 0;
+          rc[u] = (uint32_t)r | ((uint32_t)(r + e) << 16);
+        } else {
+          rc[u] = 0xffffffffu;
+        }
         acc[u] = 0.0;
       }
-      for (int a = 0; a < g.px; ++a)
-        for (int bb = 0; bb < g.py; ++bb) {
-          __syncthreads();
-          const float* src = xc + voxel_row(g, cx + a, cy + bb, cz) * n;
-          for (int e = tid; e < g.pz * n; e += nth) run[e] = src[e];
-          __syncthreads();
+      __syncthreads();  // the run buffers are free
+      {
+        const float* src = run_src(0);
+        for (int e = tid; e < runlen; e += nth) runs[e] = src[e];
+      }
+      __syncthreads();
+      for (int q = 0; q < nruns; ++q) {
+        const float* cur = runs + (size_t)(q & 1) * runlen;
+        float pre[kRefinePrefetch];
+        if (prefetch && q + 1 < nruns) {
+          const float* src = run_src(q + 1);
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            if (!live[u]) continue;
-            double s_ = acc[u];
-            for (int rr = 0; rr < g.pz; ++rr) s_ = fma((double)run[rr * n + ei[u]], (double)run[rr * n + ej[u]], s_);
-            acc[u] = s_;
+          for (int i = 0; i < kRefinePrefetch; ++i) {
+            const int e = tid + i * nth;
+            pre[i] = e < runlen ? src[e] : 0.f;
           }
         }
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        if (!live[u]) continue;
-        A[ei[u] * lda + ej[u]] = acc[u];
-        A[ej[u] * lda + ei[u]] = acc[u];
+        for (int u = 0; u < kRefineEntries; ++u) {
+          if (rc[u] == 0xffffffffu) continue;
+          const int r = (int)(rc[u] & 0xffffu), c = (int)(rc[u] >> 16);
+          double s_ = acc[u];
+          for (int rr = 0; rr < g.pz; ++rr) s_ = fma((double)cur[rr * n + r], (double)cur[rr * n + c], s_);
+          acc[u] = s_;
+        }
+        if (q + 1 < nruns) {
+          float* nxt = runs + (size_t)((q + 1) & 1) * runlen;
+          if (prefetch) {
+#pragma unroll
+            for (int i = 0; i < kRefinePrefetch; ++i) {
+              const int e = tid + i * nth;
+              if (e < runlen) nxt[e] = pre[i];
+            }
+          } else {
+            __syncthreads();  // everyone is done with the previous use of nxt
+            const float* src = run_src(q + 1);
+            for (int e = tid; e < runlen; e += nth) nxt[e] = src[e];
+          }
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int u = 0; u < kRefineEntries; ++u) {
+        if (rc[u] == 0xffffffffu) continue;
+        const int r = (int)(rc[u] & 0xffffu), c = (int)(rc[u] >> 16);
+        A[r * lda + c] = acc[u];
+        A[c * lda + r] = acc[u];
       }
     }
     __syncthreads();
-    if (n > 64 && nth == 128)
-      eigh_mp_block<double>(A, red, n, g.nvox_patch, vecs + pid * (long long)n * n,
-                            lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid,
-                            sig2 ? sig2 + pid : nullptr);
-    else if (tid < 32)
-      eigh_mp_warp<double>(A, n, g.nvox_patch, vecs + pid * (long long)n * n,
-                           lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid,
-                           sig2 ? sig2 + pid : nullptr);
+    eigh_mp_block<double>(A, red, n, g.nvox_patch, vecs + pid * (long long)n * n,
+                          lam_out ? lam_out + pid * n : nullptr, ranks + pid, wgt + pid,
+                          sig2 ? sig2 + pid : nullptr);
     __syncthreads();
   }
 }
