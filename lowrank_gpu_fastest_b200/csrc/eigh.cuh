@@ -105,83 +105,6 @@ __host__ __device__ inline size_t eigh_smem_elems(int n) {
   return (size_t)n * eigh_lda(n) + (size_t)n * kLdy + 5 * (size_t)n + (size_t)4 * n * kInvGroup;
 }
 
-// Sturm counts of two shifts at once (two independent dependency chains per lane).
-template <typename Real>
-__device__ __forceinline__ void sturm_count2(const Real* __restrict__ d, const Real* __restrict__ e2, int n, Real x0,
-                                             Real x1, Real pivmin, int& c0, int& c1) {
-  Real q0 = d[0] - x0, q1 = d[0] - x1;
-  if (fabs(q0) < pivmin) q0 = -pivmin;
-  if (fabs(q1) < pivmin) q1 = -pivmin;
-  int a0 = q0 < Real(0), a1 = q1 < Real(0);
-  for (int i = 1; i < n; ++i) {
-    const Real di = d[i], ei = e2[i - 1];
-    q0 = (di - x0) - Num<Real>::fdiv(ei, q0);
-    q1 = (di - x1) - Num<Real>::fdiv(ei, q1);
-    if (fabs(q0) < pivmin) q0 = -pivmin;
-    if (fabs(q1) < pivmin) q1 = -pivmin;
-    a0 += q0 < Real(0);
-    a1 += q1 < Real(0);
-  }
-  c0 = a0;
-  c1 = a1;
-}
-
-// All eigenvalues of the symmetric tridiagonal (d, e) (e2 = e^2) by bisection
-// on Sturm counts, ascending into lam; two chains per lane. Returns the
-// Gerschgorin norm bound in tnorm. One warp.
-template <typename Real>
-__device__ void bisect_all(const Real* d, const Real* e, const Real* e2, Real* lam, int n, Real& tnorm_out) {
-  const int lane = threadIdx.x & 31;
-  const Real eps = Num<Real>::eps();
-  Real glo = Num<Real>::huge(), ghi = -Num<Real>::huge();
-  for (int i = lane; i < n; i += 32) {
-    const Real r = (i > 0 ? fabs(e[i - 1]) : Real(0)) + (i < n - 1 ? fabs(e[i]) : Real(0));
-    glo = fmin(glo, d[i] - r);
-    ghi = fmax(ghi, d[i] + r);
-  }
-  glo = warp_min(glo);
-  ghi = warp_max(ghi);
-  const Real tnorm = fmax(fmax(fabs(glo), fabs(ghi)), Num<Real>::tiny());
-  glo -= Real(4) * eps * tnorm * n;
-  ghi += Real(4) * eps * tnorm * n;
-  const Real pivmin = Num<Real>::tiny() * Real(4);
-  const Real abstol = Real(0.1) * eps * tnorm;
-  __syncwarp();
-  for (int j0 = lane; j0 < n; j0 += 64) {
-    const int j1 = j0 + 32;
-    const bool has1 = j1 < n;
-    Real lo0 = glo, hi0 = ghi, lo1 = glo, hi1 = ghi;
-    bool run0 = true, run1 = has1;
-    for (int it = 0; it < 200 && (run0 || run1); ++it) {
-      if (run0) {
-        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo0), fabs(hi0)));
-        const Real mid = Real(0.5) * (lo0 + hi0);
-        run0 = hi0 - lo0 > tol && mid > lo0 && mid < hi0;
-      }
-      if (run1) {
-        const Real tol = fmax(abstol, Real(2) * eps * fmax(fabs(lo1), fabs(hi1)));
-        const Real mid = Real(0.5) * (lo1 + hi1);
-        run1 = hi1 - lo1 > tol && mid > lo1 && mid < hi1;
-      }
-      if (!run0 && !run1) break;
-      const Real m0 = Real(0.5) * (lo0 + hi0), m1 = Real(0.5) * (lo1 + hi1);
-      int c0, c1;
-      sturm_count2(d, e2, n, m0, m1, pivmin, c0, c1);
-      if (run0) {
-        if (c0 > j0) hi0 = m0; else lo0 = m0;
-      }
-      if (run1) {
-        if (c1 > j1) hi1 = m1; else lo1 = m1;
-      }
-    }
-    lam[j0] = Real(0.5) * (lo0 + hi0);
-    if (has1) lam[j1] = Real(0.5) * (lo1 + hi1);
-  }
-  __syncwarp();
-
-  tnorm_out = tnorm;
-}
-
 // MP rank from the ascending eigenvalues lam * unscale, evaluated like
 // step0_numpy_loop.py:18-24 (float32 eigs and suffix sums, float64 test,
 // a count over all indices); W holds 2n floats of scratch. Returns the
@@ -233,267 +156,19 @@ __device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float*
   return margin;
 }
 
-// One warp: eigen-decomposition of the symmetric n x n matrix the caller put
-// in the first n*lda elements of ``sm``, MP rank and weight, top-p
-// eigenvectors (rows of the compact p x n block ``V``), optionally the
-// ascending eigenvalues. Returns the smallest |lhs/rhs - 1| of the MP test.
-template <typename Real>
-__device__ double eigh_mp_warp(Real* sm, int n, int nvox, float* V, float* lam_out, int32_t* rank_out,
-                               float* w_out, float* s2_out) {
-  const int lane = threadIdx.x & 31;
-  const int lda = eigh_lda(n);
-  Real* A = sm;                  // n x lda, symmetric working matrix
-  Real* Y = A + n * lda;         // n x kLdy, current chunk of eigenvectors
-  Real* d = Y + n * kLdy;        // tridiagonal diagonal
-  Real* e = d + n;               // sub-diagonal e[0..n-2]
-  Real* e2 = e + n;              // e^2
-  Real* tau = e2 + n;            // reflector scalars
-  Real* lam = tau + n;           // ascending eigenvalues (scaled)
-  Real* W = lam + n;             // scratch: 4 * n * kInvGroup elements
-  const Real eps = Num<Real>::eps();
-
-  // ---- exact power-of-two scaling -------------------------------------------
-  Real dmax = 0;
-  for (int i = lane; i < n; i += 32) dmax = fmax(dmax, fabs(A[i * lda + i]));
-  dmax = warp_max(dmax);
-  int ex = 0;
-  if (dmax > Real(0) && isfinite(dmax)) frexp(dmax, &ex);
-  const Real scale = ldexp(Real(1), -ex), unscale = ldexp(Real(1), ex);
-  for (int idx = lane; idx < n * n; idx += 32) {
-    const int r = idx / n, c = idx - r * n;
-    A[r * lda + c] *= scale;
-  }
-  __syncwarp();
-
-  // ---- Householder tridiagonalisation ---------------------------------------
-  Real* vv = W;
-  Real* pp = W + n;
-  Real* ww = W + 2 * n;
-  for (int k = 0; k < n - 2; ++k) {
-    const int L = n - k - 1;
-    Real part = 0;
-    for (int i = 1 + lane; i < L; i += 32) {
-      const Real v = A[(k + 1 + i) * lda + k];
-      part = fma(v, v, part);
-    }
-    const Real xnorm2 = warp_sum(part);
-    const Real alpha = A[(k + 1) * lda + k];
-    Real taui = 0, beta = alpha;
-    if (xnorm2 > Real(0)) {
-      beta = -copysign(sqrt(fma(alpha, alpha, xnorm2)), alpha);
-      taui = (beta - alpha) / beta;
-      const Real sc = Real(1) / (alpha - beta);
-      for (int i = 1 + lane; i < L; i += 32) A[(k + 1 + i) * lda + k] *= sc;
-    }
-    if (lane == 0) {
-      e[k] = beta;
-      d[k] = A[k * lda + k];
-      tau[k] = taui;
-    }
-    __syncwarp();
-    if (taui != Real(0)) {
-      for (int i = lane; i < L; i += 32) vv[i] = (i == 0) ? Real(1) : A[(k + 1 + i) * lda + k];
-      __syncwarp();
-      for (int i = lane; i < L; i += 32) {
-        const Real* row = A + (k + 1 + i) * lda + (k + 1);
-        Real s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        int j = 0;
-        for (; j + 4 <= L; j += 4) {
-          s0 = fma(row[j], vv[j], s0);
-          s1 = fma(row[j + 1], vv[j + 1], s1);
-          s2 = fma(row[j + 2], vv[j + 2], s2);
-          s3 = fma(row[j + 3], vv[j + 3], s3);
-        }
-        for (; j < L; ++j) s0 = fma(row[j], vv[j], s0);
-        pp[i] = taui * ((s0 + s1) + (s2 + s3));
-      }
-      __syncwarp();
-      Real part2 = 0;
-      for (int i = lane; i < L; i += 32) part2 = fma(pp[i], vv[i], part2);
-      const Real kc = Real(-0.5) * taui * warp_sum(part2);
-      for (int i = lane; i < L; i += 32) ww[i] = fma(kc, vv[i], pp[i]);
-      __syncwarp();
-      for (int i = lane; i < L; i += 32) {
-        const Real vi = vv[i], wi = ww[i];
-        Real* row = A + (k + 1 + i) * lda + (k + 1);
-        for (int j = 0; j < L; ++j) row[j] = fma(-vi, ww[j], fma(-wi, vv[j], row[j]));
-      }
-      __syncwarp();
-    }
-  }
-  if (lane == 0) {
-    if (n >= 2) {
-      d[n - 2] = A[(n - 2) * lda + (n - 2)];
-      e[n - 2] = A[(n - 1) * lda + (n - 2)];
-      tau[n - 2] = 0;
-    }
-    d[n - 1] = A[(n - 1) * lda + (n - 1)];
-    e[n - 1] = 0;
-    tau[n - 1] = 0;
-  }
-  __syncwarp();
-  for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : Real(0);
-
-  Real tnorm;
-  bisect_all<Real>(d, e, e2, lam, n, tnorm);
-  int p;
-  const double margin = mp_rank<Real>(lam, unscale, n, nvox, reinterpret_cast<float*>(W), p, s2_out);
-  if (lane == 0) {
-    *rank_out = p;
-    *w_out = (float)(1.0 / (2.0 + (double)p));
-  }
-  if (lam_out != nullptr)
-    for (int i = lane; i < n; i += 32) lam_out[i] = (float)(lam[i] * unscale);
-  if (p == 0) return margin;
-  __syncwarp();
-
-  // ---- top-p eigenvectors, in chunks of kInvGroup ---------------------------
-  // Each chunk: inverse iteration on the tridiagonal (one lane per vector),
-  // Householder back-transform (one lane per vector), then modified
-  // Gram-Schmidt in descending eigenvalue order against the vectors already
-  // written (earlier chunks, read back from the output) and the chunk's
-  // earlier vectors; the chunk is then written to the output, eigenvector k
-  // as row k of a compact p x n block.
-  const Real pivtol = eps * tnorm;
-  Real* RU0 = W;                     // reciprocal pivots
-  Real* U1 = RU0 + n * kInvGroup;    // first super-diagonal of U
-  Real* ML = U1 + n * kInvGroup;     // multipliers
-  Real* SW = ML + n * kInvGroup;     // row swaps (U's second super-diagonal is e[i+1] there)
-  for (int j0 = 0; j0 < p; j0 += kInvGroup) {
-    const int g = min(kInvGroup, p - j0);
-    if (lane < g) {
-      const int q = lane;
-      const int j = j0 + q;  // descending index
-      const Real sig = lam[n - 1 - j];
-      Real c = d[0] - sig, s = (n > 1) ? e[0] : Real(0);
-      for (int i = 0; i < n - 1; ++i) {
-        const Real ei = e[i];
-        const Real an = d[i + 1] - sig;
-        const Real en = (i + 1 < n - 1) ? e[i + 1] : Real(0);
-        Real piv;
-        if (fabs(c) >= fabs(ei)) {
-          const Real m = (ei == Real(0)) ? Real(0) : ei / c;
-          piv = c;
-          U1[i * kInvGroup + q] = s;
-          ML[i * kInvGroup + q] = m;
-          SW[i * kInvGroup + q] = 0;
-          c = fma(-m, s, an);
-          s = en;
-        } else {
-          const Real m = c / ei;
-          piv = ei;
-          U1[i * kInvGroup + q] = an;
-          ML[i * kInvGroup + q] = m;
-          SW[i * kInvGroup + q] = 1;
-          c = fma(-m, an, s);
-          s = -m * en;
-        }
-        if (fabs(piv) < pivtol) piv = (piv < Real(0)) ? -pivtol : pivtol;
-        RU0[i * kInvGroup + q] = Real(1) / piv;
-      }
-      if (fabs(c) < pivtol) c = (c < Real(0)) ? -pivtol : pivtol;
-      RU0[(n - 1) * kInvGroup + q] = Real(1) / c;
-      for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
-      for (int iter = 0; iter < 3; ++iter) {
-        for (int i = 0; i < n - 1; ++i) {
-          const Real bi = Y[i * kLdy + q], bi1 = Y[(i + 1) * kLdy + q];
-          const Real m = ML[i * kInvGroup + q];
-          if (SW[i * kInvGroup + q] != Real(0)) {
-            Y[i * kLdy + q] = bi1;
-            Y[(i + 1) * kLdy + q] = fma(-m, bi1, bi);
-          } else {
-            Y[(i + 1) * kLdy + q] = fma(-m, bi, bi1);
-          }
-        }
-        Real x2 = Y[(n - 1) * kLdy + q] * RU0[(n - 1) * kInvGroup + q];
-        Y[(n - 1) * kLdy + q] = x2;
-        Real x1 = x2, amax = fabs(x2);
-        if (n >= 2) {
-          x1 = (Y[(n - 2) * kLdy + q] - U1[(n - 2) * kInvGroup + q] * x2) * RU0[(n - 2) * kInvGroup + q];
-          Y[(n - 2) * kLdy + q] = x1;
-          amax = fmax(amax, fabs(x1));
-        }
-        for (int i = n - 3; i >= 0; --i) {
-          const Real u2 = (SW[i * kInvGroup + q] != Real(0)) ? e[i + 1] : Real(0);
-          const Real xi = (Y[i * kLdy + q] - U1[i * kInvGroup + q] * x1 - u2 * x2) * RU0[i * kInvGroup + q];
-          Y[i * kLdy + q] = xi;
-          amax = fmax(amax, fabs(xi));
-          x2 = x1;
-          x1 = xi;
-        }
-        // normalise with a max-abs prescale (the solve can grow by 1/pivtol per
-        // tiny pivot); a non-finite solve restarts from a fresh start vector
-        if (!(amax > Real(0)) || !isfinite(amax)) {
-          for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
-          continue;
-        }
-        const Real sa = Real(1) / amax;
-        Real nrm = 0;
-        for (int i = 0; i < n; ++i) {
-          const Real v = Y[i * kLdy + q] * sa;
-          Y[i * kLdy + q] = v;
-          nrm = fma(v, v, nrm);
-        }
-        const Real inv = Num<Real>::rsq(nrm);
-        for (int i = 0; i < n; ++i) Y[i * kLdy + q] *= inv;
-      }
-      // back-transform: x = H(0) H(1) ... H(n-3) y
-      for (int k = n - 3; k >= 0; --k) {
-        const Real tk = tau[k];
-        if (tk == Real(0)) continue;
-        const int L = n - k - 1;
-        Real dot = Y[(k + 1) * kLdy + q];
-        for (int i = 1; i < L; ++i) dot = fma(A[(k + 1 + i) * lda + k], Y[(k + 1 + i) * kLdy + q], dot);
-        const Real f = tk * dot;
-        Y[(k + 1) * kLdy + q] -= f;
-        for (int i = 1; i < L; ++i)
-          Y[(k + 1 + i) * kLdy + q] = fma(-f, A[(k + 1 + i) * lda + k], Y[(k + 1 + i) * kLdy + q]);
-      }
-    }
-    __syncwarp();
-    // modified Gram-Schmidt, then write the chunk
-    for (int q = 0; q < g; ++q) {
-      const int j = j0 + q;
-      for (int i = 0; i < j; ++i) {
-        Real part = 0;
-        if (i < j0) {
-          for (int r = lane; r < n; r += 32) part = fma((Real)V[i * n + r], Y[r * kLdy + q], part);
-        } else {
-          for (int r = lane; r < n; r += 32) part = fma(Y[r * kLdy + (i - j0)], Y[r * kLdy + q], part);
-        }
-        const Real dot = warp_sum(part);
-        if (i < j0) {
-          for (int r = lane; r < n; r += 32) Y[r * kLdy + q] = fma(-dot, (Real)V[i * n + r], Y[r * kLdy + q]);
-        } else {
-          for (int r = lane; r < n; r += 32) Y[r * kLdy + q] = fma(-dot, Y[r * kLdy + (i - j0)], Y[r * kLdy + q]);
-        }
-        __syncwarp();
-      }
-      Real part = 0;
-      for (int r = lane; r < n; r += 32) part = fma(Y[r * kLdy + q], Y[r * kLdy + q], part);
-      const Real inv = Num<Real>::rsq(fmax(warp_sum(part), Num<Real>::tiny()));
-      for (int r = lane; r < n; r += 32) Y[r * kLdy + q] *= inv;
-      __syncwarp();
-    }
-    for (int idx = lane; idx < n * g; idx += 32) {
-      const int c = idx / n, r = idx - c * n;
-      V[(j0 + c) * n + r] = (float)Y[r * kLdy + c];
-    }
-    __syncwarp();
-  }
-  return margin;
-}
-
-// One CTA of 128 threads: the same decomposition as eigh_mp_warp<Real> for
-// the float64 pass at T > 64, where one warp per matrix leaves a near-tie's
-// refinement (a single wave of such solves) far behind the main pass. The
-// matrix stays in shared memory (odd row stride: a warp's threads, one row
-// each, hit distinct banks); thread i owns row i of the trailing block in the
-// Householder steps, the two dot products per step are block reductions;
-// thread j bisects eigenvalue j; inverse iteration (one lane per vector),
-// the back-transform (warp w: vectors w and w + 4) and Gram-Schmidt follow
-// eigh_mp_warp. ``red`` = 8 elements of scratch. Returns the MP margin (all
-// threads).
+// One CTA of 128 threads, any n <= 128: eigen-decomposition of the symmetric
+// n x n matrix the caller put in the first n*lda elements of ``sm`` (used in
+// float64 by the near-tie pass), MP rank and weight, top-p eigenvectors (rows
+// of the compact p x n block ``V``), optionally the ascending eigenvalues.
+// Exact power-of-two scaling; Householder tridiagonalisation with the matrix
+// in shared memory (odd row stride: a warp's threads, one row each, hit
+// distinct banks), thread i owning row i of the trailing block, the two dot
+// products per step block reductions; thread j bisects eigenvalue j on
+// Sturm counts; the MP test on warp 0; inverse iteration on the tridiagonal
+// (one lane per vector, partial pivoting), the back-transform (warp w:
+// vectors w and w + 4) and modified Gram-Schmidt in descending eigenvalue
+// order against the vectors already written. ``red`` = 8 elements of
+// scratch. Returns the MP margin (warp 0; 0 on the other warps).
 template <typename Real>
 __device__ Real block_sum128(Real v, Real* red) {
   v = warp_sum(v);

@@ -72,7 +72,8 @@ __device__ __forceinline__ float cta_min(float v, float* red) {
   return s;
 }
 
-// Eigenvalues of the tridiagonal below x (one chain), sturm_count2's arithmetic.
+// Eigenvalues of the tridiagonal below x (one chain): sturm2_reg's pivot
+// recurrence (eigh_reg.cuh) on the tridiagonal in shared memory.
 __device__ __forceinline__ int sturm_count1(const float* __restrict__ d, const float* __restrict__ e2, int n, float x,
                                             float pivmin) {
   float q = d[0] - x;

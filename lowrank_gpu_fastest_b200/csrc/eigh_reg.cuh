@@ -1,8 +1,9 @@
 // Register-resident float32 eigensolver for T <= TMAX (TMAX in {32, 48, 64}).
 //
-// Same algorithm as eigh_mp_warp<float> (eigh.cuh) - Householder
-// tridiagonalisation, bisection, MP rank, inverse iteration, back-transform,
-// Gram-Schmidt - with the data placed for a warp:
+// One warp per matrix: Householder tridiagonalisation, bisection on Sturm
+// counts, MP rank (mp_rank, eigh.cuh), inverse iteration, back-transform,
+// Gram-Schmidt (the steps of eigh_mp_block, eigh.cuh), with the data placed
+// for a warp:
 //
 //  * lane l holds rows l and l + 32 of the working matrix in registers
 //    (a[NR][TMAX], every column index compile-time), so the reflector's
@@ -17,9 +18,7 @@
 //  * the back-transform and the Gram-Schmidt pass work on row-distributed
 //    vectors with warp reductions, 8 vectors at a time.
 //
-// The arithmetic follows the shared-memory routine up to the order of the
-// float32 sums, so the results agree to float32 round-off, and the same
-// near-tie test queues patches for the float64 pass.
+// The near-tie test (mp_rank's margin) queues patches for the float64 pass.
 #pragma once
 
 #include "eigh.cuh"
@@ -51,7 +50,9 @@ __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
 // Sturm counts (eigenvalues below x0 and x1) of the tridiagonal held in
 // registers: dr[i] = d_i, e2r[i] = e_i^2. Entries i >= n are padded with
 // d_i = +big, e_i = 0, which adds positive pivots only, so the counts equal
-// the n x n ones; for i < n the arithmetic is sturm_count2's.
+// the n x n ones. The pivots follow q_i = (d_i - x) - e_{i-1}^2 / q_{i-1}, a
+// pivot smaller than pivmin in magnitude replaced by -pivmin; the count is
+// the number of negative pivots.
 template <int TMAX>
 __device__ __forceinline__ void sturm2_reg(const float (&dr)[TMAX], const float (&e2r)[TMAX], float x0, float x1,
                                            float pivmin, int& c0, int& c1) {
@@ -73,9 +74,9 @@ __device__ __forceinline__ void sturm2_reg(const float (&dr)[TMAX], const float 
 }
 
 // All eigenvalues of the tridiagonal (d, e, e2 in shared memory) ascending
-// into lam; tnorm = Gerschgorin bound. bisect_all's bisection (same interval
-// rule and stopping test) with the tridiagonal in registers and one
-// multisection pass first: the 64 chains evaluate counts at 64 evenly spaced
+// into lam; tnorm = Gerschgorin bound. Bisection (an interval [lo, hi] with
+// count(lo) <= j < count(hi), stopped at max(0.1 eps tnorm, 2 eps |lambda|))
+// with the tridiagonal in registers and one multisection pass first: the 64 chains evaluate counts at 64 evenly spaced
 // interior points of the Gerschgorin interval, and every chain starts from
 // the two neighbouring points that bracket its eigenvalue (six bisection
 // steps for the price of one).
