@@ -13,8 +13,8 @@
 //  * the reflector vectors are kept in shared memory (HV, one row per step,
 //    zero above the sub-diagonal and 1 on it) and double as the broadcast
 //    buffer of the matrix-vector product;
-//  * inverse iteration keeps its vector in registers (loops over the
-//    tridiagonal unrolled to TMAX), the LU factors in shared memory;
+//  * inverse iteration keeps its vector and the LU factors in shared memory
+//    (one lane per eigenvector);
 //  * the back-transform and the Gram-Schmidt pass work on row-distributed
 //    vectors with warp reductions, 8 vectors at a time.
 //
@@ -371,51 +371,47 @@ __global__ void __launch_bounds__(32)
       }
       if (fabsf(c) < pivtol) c = (c < 0.f) ? -pivtol : pivtol;
       RU0[(n - 1) * kInvGroup + q] = __fdividef(1.f, c);
-      float y[TMAX];
-#pragma unroll
-      for (int i = 0; i < TMAX; ++i) y[i] = (i < n) ? start_entry(i, j) : 0.f;
+      // the vector in shared memory (Yt column q)
+      float* Y = Yt;
+      for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
       for (int iter = 0; iter < 3; ++iter) {
-#pragma unroll
-        for (int i = 0; i < TMAX - 1; ++i) {
-          if (i < n - 1) {
-            const float m = ML[i * kInvGroup + q];
-            const bool sw = SW[i * kInvGroup + q] != 0.f;
-            const float yi = y[i], yn = y[i + 1];
-            y[i] = sw ? yn : yi;
-            y[i + 1] = sw ? fmaf(-m, yn, yi) : fmaf(-m, yi, yn);
-          }
+        for (int i = 0; i < n - 1; ++i) {
+          const float yi = Y[i * kLdy + q], yn = Y[(i + 1) * kLdy + q];
+          const float m = ML[i * kInvGroup + q];
+          const bool sw = SW[i * kInvGroup + q] != 0.f;
+          Y[i * kLdy + q] = sw ? yn : yi;
+          Y[(i + 1) * kLdy + q] = sw ? fmaf(-m, yn, yi) : fmaf(-m, yi, yn);
         }
-        float amax = 0.f;
-#pragma unroll
-        for (int i = TMAX - 1; i >= 0; --i) {
-          if (i < n) {
-            const float y1 = (i + 1 < n && i + 1 < TMAX) ? y[(i + 1) % TMAX] : 0.f;
-            const float y2 = (i + 2 < n && i + 2 < TMAX) ? y[(i + 2) % TMAX] : 0.f;
-            const float u2 = (i + 1 < n - 1 && SW[i * kInvGroup + q] != 0.f) ? e[i + 1] : 0.f;
-            const float u1 = (i < n - 1) ? U1[i * kInvGroup + q] : 0.f;
-            y[i] = (y[i] - u1 * y1 - u2 * y2) * RU0[i * kInvGroup + q];
-            amax = fmaxf(amax, fabsf(y[i]));
-          }
+        float x2 = Y[(n - 1) * kLdy + q] * RU0[(n - 1) * kInvGroup + q];
+        Y[(n - 1) * kLdy + q] = x2;
+        float x1 = x2, amax = fabsf(x2);
+        if (n >= 2) {
+          x1 = (Y[(n - 2) * kLdy + q] - U1[(n - 2) * kInvGroup + q] * x2) * RU0[(n - 2) * kInvGroup + q];
+          Y[(n - 2) * kLdy + q] = x1;
+          amax = fmaxf(amax, fabsf(x1));
+        }
+        for (int i = n - 3; i >= 0; --i) {
+          const float u2 = (SW[i * kInvGroup + q] != 0.f) ? e[i + 1] : 0.f;
+          const float xi = (Y[i * kLdy + q] - U1[i * kInvGroup + q] * x1 - u2 * x2) * RU0[i * kInvGroup + q];
+          Y[i * kLdy + q] = xi;
+          amax = fmaxf(amax, fabsf(xi));
+          x2 = x1;
+          x1 = xi;
         }
         if (!(amax > 0.f) || !isfinite(amax)) {
-#pragma unroll
-          for (int i = 0; i < TMAX; ++i) y[i] = (i < n) ? start_entry(i, j + 977 * (iter + 1)) : 0.f;
+          for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
           continue;
         }
         const float sa = 1.f / amax;
         float nrm = 0.f;
-#pragma unroll
-        for (int i = 0; i < TMAX; ++i) {
-          y[i] *= sa;
-          nrm = fmaf(y[i], y[i], nrm);
+        for (int i = 0; i < n; ++i) {
+          const float v = Y[i * kLdy + q] * sa;
+          Y[i * kLdy + q] = v;
+          nrm = fmaf(v, v, nrm);
         }
         const float inv = rsqrtf(nrm);
-#pragma unroll
-        for (int i = 0; i < TMAX; ++i) y[i] *= inv;
+        for (int i = 0; i < n; ++i) Y[i * kLdy + q] *= inv;
       }
-#pragma unroll
-      for (int i = 0; i < TMAX; ++i)
-        if (i < n) Yt[i * kLdy + q] = y[i];
     }
     __syncwarp();
     LRD_STAMP(5);
