@@ -500,9 +500,9 @@ __device__ double eigh_mp_block(Real* sm, Real* red, int n, int nvox, float* V, 
 }
 
 // Shared memory bytes of eigh_refine_kernel: the float64 eigensolver's arrays
-// plus two staged z-runs of the patch (pz*T floats each).
+// plus two staged z-runs of the patch (pz*T values each, held as float64).
 __host__ __device__ inline size_t eigh_refine_smem_bytes(int n, int pz) {
-  return sizeof(double) * (eigh_smem_elems(n) + 8) + 2 * sizeof(float) * (size_t)pz * n;
+  return sizeof(double) * (eigh_smem_elems(n) + 8) + 2 * sizeof(double) * (size_t)pz * n;
 }
 
 constexpr int kRefineEntries = 24;  // Gram entries per thread per pass over the patch
@@ -514,7 +514,9 @@ constexpr int kRefinePrefetch = 16; // floats of the next z-run a thread prefetc
 // patch per block at a time (128 threads). The block forms G = Xc^T Xc in
 // float64 (products of the float32 centred values are exact in float64, the
 // sum is float64) in passes of kRefineEntries entries per thread over the
-// patch's z-runs, the next run prefetched through registers into a second
+// patch's z-runs, each run converted to float64 once as it is staged (the
+// conversions inside the product loop bound this step: 1.6 M cycles at
+// T = 64) and the next run prefetched through registers into a second
 // buffer; then the block's float64 eigensolver (eigh_mp_block) overwrites the
 // patch's rank, weight, eigenvectors (and eigenvalues if requested). A queue
 // holds a handful of patches per volume, so this pass is one patch's latency:
@@ -528,7 +530,7 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
   const int lda = eigh_lda(n);
   double* A = sm_ref;
   double* red = sm_ref + eigh_smem_elems(n);  // block reductions
-  float* runs = reinterpret_cast<float*>(red + 8);  // two z-run buffers
+  double* runs = red + 8;  // two z-run buffers, converted to float64 once when staged
   const int runlen = g.pz * n;
   const int count = refine_count[0];
   const int first = refine_count[1];
@@ -567,11 +569,11 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
       __syncthreads();  // the run buffers are free
       {
         const float* src = run_src(0);
-        for (int e = tid; e < runlen; e += nth) runs[e] = src[e];
+        for (int e = tid; e < runlen; e += nth) runs[e] = (double)src[e];
       }
       __syncthreads();
       for (int q = 0; q < nruns; ++q) {
-        const float* cur = runs + (size_t)(q & 1) * runlen;
+        const double* cur = runs + (size_t)(q & 1) * runlen;
         float pre[kRefinePrefetch];
         if (prefetch && q + 1 < nruns) {
           const float* src = run_src(q + 1);
@@ -586,21 +588,21 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
           if (rc[u] == 0xffffffffu) continue;
           const int r = (int)(rc[u] & 0xffffu), c = (int)(rc[u] >> 16);
           double s_ = acc[u];
-          for (int rr = 0; rr < g.pz; ++rr) s_ = fma((double)cur[rr * n + r], (double)cur[rr * n + c], s_);
+          for (int rr = 0; rr < g.pz; ++rr) s_ = fma(cur[rr * n + r], cur[rr * n + c], s_);
           acc[u] = s_;
         }
         if (q + 1 < nruns) {
-          float* nxt = runs + (size_t)((q + 1) & 1) * runlen;
+          double* nxt = runs + (size_t)((q + 1) & 1) * runlen;
           if (prefetch) {
 #pragma unroll
             for (int i = 0; i < kRefinePrefetch; ++i) {
               const int e = tid + i * nth;
-              if (e < runlen) nxt[e] = pre[i];
+              if (e < runlen) nxt[e] = (double)pre[i];
             }
           } else {
             __syncthreads();  // everyone is done with the previous use of nxt
             const float* src = run_src(q + 1);
-            for (int e = tid; e < runlen; e += nth) nxt[e] = src[e];
+            for (int e = tid; e < runlen; e += nth) nxt[e] = (double)src[e];
           }
         }
         __syncthreads();
