@@ -297,3 +297,19 @@ def test_host_pipeline_with_patch_batches(cuda_ok):
     dev, dr = run_dev(vol, (5, 5, 5), 2)
     np.testing.assert_array_equal(hr, dr)
     np.testing.assert_array_equal(host, dev)
+
+
+@pytest.mark.parametrize("T", [30, 37, 101])
+def test_frame_counts_off_the_column_kernel(cuda_ok, T):
+    """T not a multiple of 4 takes the per-patch Gram kernel (the column and
+    tensor Grams need T % 4 == 0); against the live step-0 loop."""
+    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+
+    shape, patch, stride = (12, 11, 10, T), (5, 5, 5), 2
+    vol = make_phantom_lowrank(shape, seed=4)[0]
+    ref, ref_ranks = orc.denoise(vol, patch, stride)
+    for form in ("plain", "accurate", "tensor"):
+        out, ranks = run_dev(vol, patch, stride, form=form)
+        np.testing.assert_array_equal(ranks, ref_ranks)
+        tol = PLAIN_TOL if form == "plain" else 4e-7  # accurate/tensor follow float64, step 0 is ~2e-7 away
+        assert rel_l2(out, ref) <= tol, (form, rel_l2(out, ref))
