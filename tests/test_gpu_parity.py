@@ -313,3 +313,18 @@ def test_frame_counts_off_the_column_kernel(cuda_ok, T):
         np.testing.assert_array_equal(ranks, ref_ranks)
         tol = PLAIN_TOL if form == "plain" else 4e-7  # accurate/tensor follow float64, step 0 is ~2e-7 away
         assert rel_l2(out, ref) <= tol, (form, rel_l2(out, ref))
+
+
+@pytest.mark.parametrize("T", [2, 3, 5, 8])
+def test_few_frames_vs_live_oracle(cuda_ok, T):
+    """The shortest series (one to seven non-null eigenvalues) against the
+    live step-0 loop."""
+    rng = np.random.default_rng(T)
+    vol = (rng.standard_normal((9, 8, 7, T)) * 0.1 + np.linspace(0, 1, T)).astype(np.float32)
+    patch, stride = (3, 3, 3), 2
+    ref, ref_ranks = orc.denoise(vol, patch, stride)
+    for form in ("plain", "accurate"):
+        out, ranks = run_dev(vol, patch, stride, form=form)
+        np.testing.assert_array_equal(ranks, ref_ranks)
+        tol = PLAIN_TOL if form == "plain" else 4e-7
+        assert rel_l2(out, ref) <= tol, (form, rel_l2(out, ref))
