@@ -67,8 +67,11 @@ def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", retu
     Parameters mirror the ladder: ``patch`` (common.py:28), ``stride``
     (common.py:29), ``batch`` = patches per Gram/eigensolver launch
     (step8_tuned.py:21; ``None`` = all). ``form`` is ``"plain"`` (float32,
-    step-0 accumulation order) or ``"accurate"``. With ``return_ranks`` the
-    per-patch MP ranks (x-major patch order) are returned too.
+    step-0 accumulation order), ``"accurate"`` (float64 accumulation, close
+    to the float64 run) or ``"tensor"`` (as accurate, the Gram on the tensor
+    cores in split TF32). With ``return_ranks`` the per-patch MP ranks
+    (x-major patch order) are returned too. ``out`` (CUDA input only): a
+    preallocated output tensor of the volume's shape.
     """
     if not torch.cuda.is_available():
         raise RuntimeError("denoise needs a CUDA device (the native CUDA library is the only path)")
