@@ -236,7 +236,7 @@ void* recon_kernel_ptr(int tpt, int split, bool accurate) {
     switch (tpt) {
       case 8: return recon_fn<8, 2>(accurate);
       case 16: return recon_fn<16, 2>(accurate);
-      case 24: return recon_fn<24, 2>(accurate);
+      case 24: return accurate ? recon_fn<24, 2>(true) : (void*)lrd::recon_kernel_t24s2;
       case 32: return recon_fn<32, 2>(accurate);
       case 40: return recon_fn<40, 2>(accurate);
       case 48: return recon_fn<48, 2>(accurate);

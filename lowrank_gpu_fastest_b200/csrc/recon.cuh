@@ -74,10 +74,10 @@ struct SlabIO {
 // grid: bricks [brick0, brick0 + gridDim.x) of the nbx*nby*nbz (x-major)
 // bricks; bx*by*bz*SPLIT threads per block (<= 1024).
 template <int TPT, int SPLIT, bool ACCURATE>
-__global__ void recon_kernel(const float* __restrict__ xc, const float* __restrict__ mean,
-                             const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
-                             const float* __restrict__ wgt, float* __restrict__ out, Geom g,
-                             AxisTables tab, int brick0, SlabIO io) {
+__device__ __forceinline__ void recon_body(const float* __restrict__ xc, const float* __restrict__ mean,
+                                           const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
+                                           const float* __restrict__ wgt, float* __restrict__ out, Geom g,
+                                           AxisTables tab, int brick0, SlabIO io) {
   extern __shared__ __align__(16) float sm_recon[];
   const int T = g.nt;
   const int TP = recon_tp(T);
@@ -303,6 +303,26 @@ __global__ void recon_kernel(const float* __restrict__ xc, const float* __restri
       if (t < T) out[row * T + t] = __fdiv_rn(acc[u], den);
     }
   }
+}
+
+template <int TPT, int SPLIT, bool ACCURATE>
+__global__ void recon_kernel(const float* __restrict__ xc, const float* __restrict__ mean,
+                             const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
+                             const float* __restrict__ wgt, float* __restrict__ out, Geom g, AxisTables tab,
+                             int brick0, SlabIO io) {
+  recon_body<TPT, SPLIT, ACCURATE>(xc, mean, vecs, ranks, wgt, out, g, tab, brick0, io);
+}
+
+// The T <= 48 float32 layout (24 frames x 2 threads per voxel) with its
+// registers capped at 112: 136 by default allow 6 CTAs of 64 threads per SM,
+// 112 allow 9 (96x96x48x48 headline: 1.30 -> 1.22 ms; 96 registers spill
+// inside the patch loop and took 2.46 ms).
+__global__ void __maxnreg__(112) recon_kernel_t24s2(const float* __restrict__ xc, const float* __restrict__ mean,
+                                                    const float* __restrict__ vecs,
+                                                    const int32_t* __restrict__ ranks,
+                                                    const float* __restrict__ wgt, float* __restrict__ out, Geom g,
+                                                    AxisTables tab, int brick0, SlabIO io) {
+  recon_body<24, 2, false>(xc, mean, vecs, ranks, wgt, out, g, tab, brick0, io);
 }
 
 }  // namespace lrd
