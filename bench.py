@@ -50,6 +50,8 @@ def phase_kernel(phase, T, form):
         return "gram_tc_kernel" if (form == "tensor" and T <= 64) else "gram_z_kernel"
     if phase == "eigh_mp":
         return "eigh_reg_kernel" if T <= 64 else "eigh_cta_kernel"
+    if phase == "recon" and form == "plain" and 45 <= T <= 48:
+        return "recon_kernel_t24s2"  # 24 frames x 2 threads, built with 112 registers
     return {"center": "center_kernel", "recon": "recon_kernel"}[phase]
 
 
