@@ -111,10 +111,12 @@ int lrd_denoise(const lrd_plan* plan, const float* d_vol, float* d_out, int32_t*
  * ``h_out`` and waits. ``d_in``/``d_out`` are caller-owned device buffers of
  * the volume's size. This is the whole host->host call of step8_tuned.py:
  * 116-146 (from_numpy().cuda() ... host.copy_(...)), pipelined: the volume
- * moves in x-slabs on the plan's two copy streams, each slab's compute runs
- * on ``stream`` as soon as its planes are in, and finished output planes copy
- * out while later slabs compute (pinned host buffers make the copies
- * asynchronous). Results are identical to lrd_denoise's. */
+ * moves in x-slabs on the plan's copy streams, each slab's centring and Gram
+ * run on the plan's side streams as soon as its planes are in, its solve on
+ * ``stream``, its reconstruction on another plan stream, and finished output
+ * planes copy out while later slabs compute (pinned host buffers make the
+ * copies asynchronous). Results are identical to lrd_denoise's. The plan's
+ * streams and events make this one call at a time per plan. */
 int lrd_denoise_host(const lrd_plan* plan, const float* h_vol, float* h_out, int32_t* h_ranks,
                      float* d_in, float* d_out, int32_t* d_ranks, void* d_workspace,
                      void* stream);
