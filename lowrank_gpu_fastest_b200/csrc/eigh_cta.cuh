@@ -78,12 +78,12 @@ __device__ __forceinline__ int sturm_count1(const float* __restrict__ d, const f
                                             float pivmin) {
   float q = d[0] - x;
   if (fabsf(q) < pivmin) q = -pivmin;
-  int a = q < 0.f;
+  int a = (int)(__float_as_uint(q) >> 31);
 #pragma unroll 4
   for (int i = 1; i < n; ++i) {
     q = (d[i] - x) - __fdividef(e2[i - 1], q);
     if (fabsf(q) < pivmin) q = -pivmin;
-    a += q < 0.f;
+    a += (int)(__float_as_uint(q) >> 31);
   }
   return a;
 }
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(TMAX)
     glo -= 4.f * eps * tnorm * n;
     ghi += 4.f * eps * tnorm * n;
     const float pivmin = FLT_MIN * 4.f;
-    const float abstol = 0.1f * eps * tnorm;
+    const float abstol = eps * tnorm;  // as bisect_reg
     const float h = (ghi - glo) * (1.f / (TMAX + 1));
     int* cnt = reinterpret_cast<int*>(W);
     cnt[tid] = sturm_count1(d, e2, n, fmaf((float)(tid + 1), h, glo), pivmin);

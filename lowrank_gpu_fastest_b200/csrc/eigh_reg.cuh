@@ -52,22 +52,22 @@ __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
 // d_i = +big, e_i = 0, which adds positive pivots only, so the counts equal
 // the n x n ones. The pivots follow q_i = (d_i - x) - e_{i-1}^2 / q_{i-1}, a
 // pivot smaller than pivmin in magnitude replaced by -pivmin; the count is
-// the number of negative pivots.
+// the number of negative pivots (their sign bits: no pivot is a zero).
 template <int TMAX>
 __device__ __forceinline__ void sturm2_reg(const float (&dr)[TMAX], const float (&e2r)[TMAX], float x0, float x1,
                                            float pivmin, int& c0, int& c1) {
   float q0 = dr[0] - x0, q1 = dr[0] - x1;
   if (fabsf(q0) < pivmin) q0 = -pivmin;
   if (fabsf(q1) < pivmin) q1 = -pivmin;
-  int a0 = q0 < 0.f, a1 = q1 < 0.f;
+  int a0 = (int)(__float_as_uint(q0) >> 31), a1 = (int)(__float_as_uint(q1) >> 31);
 #pragma unroll
   for (int i = 1; i < TMAX; ++i) {
     q0 = (dr[i] - x0) - __fdividef(e2r[i - 1], q0);
     q1 = (dr[i] - x1) - __fdividef(e2r[i - 1], q1);
     if (fabsf(q0) < pivmin) q0 = -pivmin;
     if (fabsf(q1) < pivmin) q1 = -pivmin;
-    a0 += q0 < 0.f;
-    a1 += q1 < 0.f;
+    a0 += (int)(__float_as_uint(q0) >> 31);
+    a1 += (int)(__float_as_uint(q1) >> 31);
   }
   c0 = a0;
   c1 = a1;
@@ -75,7 +75,9 @@ __device__ __forceinline__ void sturm2_reg(const float (&dr)[TMAX], const float 
 
 // All eigenvalues of the tridiagonal (d, e, e2 in shared memory) ascending
 // into lam; tnorm = Gerschgorin bound. Bisection (an interval [lo, hi] with
-// count(lo) <= j < count(hi), stopped at max(0.1 eps tnorm, 2 eps |lambda|))
+// count(lo) <= j < count(hi), stopped at max(eps tnorm, 2 eps |lambda|): the
+// absolute part is LAPACK's default tolerance (eps times the norm of the
+// tridiagonal), below the float32 reduction's own error in the eigenvalues)
 // with the tridiagonal in registers and one multisection pass first: the 64 chains evaluate counts at 64 evenly spaced
 // interior points of the Gerschgorin interval, and every chain starts from
 // the two neighbouring points that bracket its eigenvalue (six bisection
@@ -97,7 +99,7 @@ __device__ __forceinline__ void bisect_reg(const float* d, const float* e, const
   glo -= 4.f * eps * tnorm * n;
   ghi += 4.f * eps * tnorm * n;
   const float pivmin = FLT_MIN * 4.f;
-  const float abstol = 0.1f * eps * tnorm;
+  const float abstol = eps * tnorm;
   const float big = 4.f * fmaxf(fabsf(glo), fabsf(ghi)) + 1.f;
   float dr[TMAX], e2r[TMAX];
 #pragma unroll
