@@ -96,12 +96,18 @@ __host__ __device__ inline int gramz_threads(int T, int ks) {
   return ((nb * (nb + 1) / 2 * ks) + 31) & ~31;
 }
 
-// grid: (columns in this launch); block: gramz_threads(T, ks) (T % 4 == 0,
-// ks in {1, 2, 4}). ``col0`` = first column (x-major index ci * ncy + cj);
-// ``gram`` points at the Gram block of the launch's first patch (patch index
-// col0 * ncz).
+// grid: nfull + (columns - nfull) * nsplit CTAs; block: gramz_threads(T, ks)
+// (T % 4 == 0, ks in {1, 2, 4}). CTA b < nfull computes every window of column
+// col0 + b; the columns after the first nfull are each cut into nsplit units
+// of consecutive windows (a unit reads only the planes of its windows), so a
+// launch whose last wave would hold a few whole columns spreads that tail
+// over many SMs. A window's planes are added in the same order either way: the
+// result does not depend on the cut. ``col0`` = first column (x-major index
+// ci * ncy + cj); ``gram`` points at the Gram block of the launch's first
+// patch (patch index col0 * ncz).
 __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g,
-                              AxisTables tab, long long col0, int ring, int ks, int* status) {
+                              AxisTables tab, long long col0, int ring, int ks, int nfull, int nsplit,
+                              int* status) {
   extern __shared__ __align__(128) float smz[];
   const int T = g.nt;
   const int rows = g.px * g.py;
@@ -116,7 +122,13 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
   const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&bars[0]);
   const uint32_t bar1 = (uint32_t)__cvta_generic_to_shared(&bars[1]);
 
-  const long long col = col0 + blockIdx.x;
+  // this CTA's column and windows [wlo, whi]
+  const int bid = (int)blockIdx.x;
+  const bool cut = bid >= nfull;
+  const int u = cut ? bid - nfull : 0, nparts = cut ? nsplit : 1, part = u % nparts;
+  const long long col = col0 + (cut ? nfull + u / nparts : bid);
+  const int wlo = part * g.ncz / nparts, whi = (part + 1) * g.ncz / nparts - 1;
+  const int zlo = tab.corners[2][wlo], zhi = tab.corners[2][whi] + g.pz - 1;  // its planes
   const int ci = (int)(col / g.ncy), cj = (int)(col % g.ncy);
   const int cx = tab.corners[0][ci], cy = tab.corners[1][cj];
   const int tid = threadIdx.x;
@@ -142,21 +154,21 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  if (tid == 0 && g.nz > 0) {
+  if (tid == 0 && zlo <= zhi) {
     mbar_expect_tx(bar0, plane_bytes);
-    tma_load_4d((uint32_t)__cvta_generic_to_shared(plane0), &xmap, bar0, 0, 0, cy, cx);
+    tma_load_4d((uint32_t)__cvta_generic_to_shared(plane0), &xmap, bar0, 0, zlo, cy, cx);
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
-  for (int z = 0; z < g.nz; ++z) {
-    const int slot = z & 1;
-    if (tid == 0 && z + 1 < g.nz) {
+  for (int z = zlo; z <= zhi; ++z) {
+    const int it = z - zlo, slot = it & 1;
+    if (tid == 0 && z + 1 <= zhi) {
       const uint32_t nb_ = slot ? bar0 : bar1;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       mbar_expect_tx(nb_, plane_bytes);
       tma_load_4d((uint32_t)__cvta_generic_to_shared(slot ? plane0 : plane1), &xmap, nb_, 0, z + 1, cy, cx);
     }
-    mbar_wait_bounded(slot ? bar1 : bar0, (uint32_t)((z >> 1) & 1), status);
-    const int klo = tab.cover[2][2 * z], khi = tab.cover[2][2 * z + 1];
+    mbar_wait_bounded(slot ? bar1 : bar0, (uint32_t)((it >> 1) & 1), status);
+    const int klo = max(tab.cover[2][2 * z], wlo), khi = min(tab.cover[2][2 * z + 1], whi);
     if (klo <= khi) {
       const float* pl = slot ? plane1 : plane0;
       float acc[16];

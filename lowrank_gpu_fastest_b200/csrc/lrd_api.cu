@@ -76,6 +76,8 @@ struct lrd_plan {
   int gramz_ring;          // window accumulator slots
   int gramz_ks = 1;        // voxel-row split per 4x4 Gram block (threads per block)
   size_t smem_gramz;
+  int gramz_slots = 0;     // column CTAs resident at once on the device (0: never cut columns)
+  int sms = 0;             // multiprocessors of the device
   size_t smem_center, smem_gram, smem_eigh, smem_recon;
   int center_warps;
   // workspace offsets (bytes)
@@ -351,8 +353,20 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
                                                                       P->tab, c0, P->gramz_ring, status);
         rc = launch_check("gram_tc_kernel launch");
       } else {
-        lrd::gram_z_kernel<<<(unsigned)nc, lrd::gramz_threads(P->g.nt, P->gramz_ks), P->smem_gramz, st>>>(
-            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, P->gramz_ks, status);
+        // A last wave of a few whole columns would leave most SMs idle while
+        // they finish: cut those columns into window ranges instead.
+        long long nfull = nc;
+        int nsplit = 1;
+        const long long slots = P->gramz_slots, rem = slots > 0 ? nc % slots : 0;
+        if (slots > 0 && nc > slots && rem > 0 && 2 * rem <= slots && P->g.ncz > 1) {
+          nsplit = (int)std::min<long long>(P->g.ncz, slots / rem);
+          if (nsplit > 1) nfull = nc - rem;
+          else nsplit = 1;
+        }
+        const long long grid = nfull + (nc - nfull) * nsplit;
+        lrd::gram_z_kernel<<<(unsigned)grid, lrd::gramz_threads(P->g.nt, P->gramz_ks), P->smem_gramz, st>>>(
+            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, P->gramz_ks, (int)nfull, nsplit,
+            status);
         rc = launch_check("gram_z_kernel launch");
       }
       if (rc) return rc;
@@ -627,6 +641,16 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     P->refine_blocks = std::max(1, std::min<int>(2 * sms, (int)std::min<long long>(g.npatch, 1 << 20)));
+    P->sms = sms;
+    int per_sm = 0;
+    if (!rc && P->use_gramz) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lrd::gram_z_kernel,
+                                                        lrd::gramz_threads(T, P->gramz_ks),
+                                                        P->smem_gramz) == cudaSuccess)
+        P->gramz_slots = per_sm * sms;
+      else
+        (void)cudaGetLastError();  // no cut columns; the launches report their own errors
+    }
   }
   if (!rc) rc = set_smem(eigh_kernel_for(T), P->smem_eigh);
   if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, false), P->smem_recon);
