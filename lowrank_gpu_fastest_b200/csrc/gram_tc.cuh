@@ -80,7 +80,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 
 // Two-stage pipeline per column CTA (256 threads): while the tensor cores
-// run plane z's MMAs (operand tiles and TMEM accumulator of stage z & 1),
+// run plane z's MMAs (operand tiles and TMEM accumulator of stage (z - zlo) & 1,
+// zlo = the CTA's first plane),
 // the CTA reads back plane z-1's Gram from the other accumulator and adds it
 // into the windows; planes arrive by TMA two ahead (two plane slots).
 //
@@ -110,11 +111,12 @@ constexpr int kGramTcThreads = 256;
 constexpr int kIssuer = 128;  // TMA + MMA issuing thread (warp 4: no TMEM readback)
 constexpr uint32_t kGramTcCols = 128;  // two accumulators of up to 64 columns
 
-// grid: (columns in this launch); block: kGramTcThreads. T <= 64, T % 4 == 0,
+// grid: nfull + (columns - nfull) * nsplit CTAs (columns cut into window
+// ranges as in gram_z_kernel); block: kGramTcThreads. T <= 64, T % 4 == 0,
 // px*py <= 128. ``gram`` points at the Gram block of patch col0 * ncz.
 __global__ void __launch_bounds__(kGramTcThreads)
     gram_tc_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g, AxisTables tab,
-                   long long col0, int ring, int* status) {
+                   long long col0, int ring, int nfull, int nsplit, int* status) {
   extern __shared__ __align__(1024) unsigned char smt[];
   const int T = g.nt;
   const int rows = g.px * g.py;
@@ -135,7 +137,13 @@ __global__ void __launch_bounds__(kGramTcThreads)
   const int warp = tid >> 5, lane = tid & 31;
   const int nth = blockDim.x;
 
-  const long long col = col0 + blockIdx.x;
+  // this CTA's column, windows [wlo, whi] and planes [zlo, zhi]
+  const int bid = (int)blockIdx.x;
+  const bool cut = bid >= nfull;
+  const int u = cut ? bid - nfull : 0, nparts = cut ? nsplit : 1, part = u % nparts;
+  const long long col = col0 + (cut ? nfull + u / nparts : bid);
+  const int wlo = part * g.ncz / nparts, whi = (part + 1) * g.ncz / nparts - 1;
+  const int zlo = tab.corners[2][wlo], zhi = tab.corners[2][whi] + g.pz - 1;
   const int ci = (int)(col / g.ncy), cj = (int)(col % g.ncy);
   const int cx = tab.corners[0][ci], cy = tab.corners[1][cj];
   const uint32_t plane_bytes = (uint32_t)(rows * T * sizeof(float));
@@ -173,18 +181,19 @@ __global__ void __launch_bounds__(kGramTcThreads)
   auto bar_mma = [&](int s) { return (uint32_t)__cvta_generic_to_shared(&bars[2 + s]); };
 
   if (tid == kIssuer) {
-    for (int z = 0; z < 2 && z < g.nz; ++z) {
-      mbar_expect_tx(bar_tma(z), plane_bytes);
-      tma_load_4d(planes_addr + (uint32_t)(z * pf * sizeof(float)), &xmap, bar_tma(z), 0, z, cy, cx);
+    for (int i = 0; i < 2 && zlo + i <= zhi; ++i) {
+      mbar_expect_tx(bar_tma(i), plane_bytes);
+      tma_load_4d(planes_addr + (uint32_t)(i * pf * sizeof(float)), &xmap, bar_tma(i), 0, zlo + i, cy, cx);
     }
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
 
-  // Reads back plane zr's Gram (accumulator zr & 1) into H and adds it into
-  // the windows it belongs to; writes out the windows it completes.
+  // Reads back plane zr's Gram (accumulator (zr - zlo) & 1) into H and adds it
+  // into the windows it belongs to; writes out the windows it completes.
   auto drain = [&](int zr) {
-    const int s = zr & 1;
-    if (!mbar_wait_bounded(bar_mma(s), (uint32_t)((zr >> 1) & 1), status, kStatusMmaTimeout)) *abort_flag = 1;
+    const int s = (zr - zlo) & 1;
+    if (!mbar_wait_bounded(bar_mma(s), (uint32_t)(((zr - zlo) >> 1) & 1), status, kStatusMmaTimeout))
+      *abort_flag = 1;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (warp < 4 && warp * 16 < T) {  // M = 64: rows 16w..16w+15 in lanes 0..15 of sub-partition w
       const int trow = warp * 16 + lane;
@@ -200,7 +209,7 @@ __global__ void __launch_bounds__(kGramTcThreads)
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();  // H complete; the accumulator is free for plane zr + 2
-    const int klo = tab.cover[2][2 * zr], khi = tab.cover[2][2 * zr + 1];
+    const int klo = max(tab.cover[2][2 * zr], wlo), khi = min(tab.cover[2][2 * zr + 1], whi);
     bool done_any = false;
     for (int e = tid; e < ntri; e += nth) {
       const uint32_t rc = tri[e];
@@ -230,10 +239,10 @@ __global__ void __launch_bounds__(kGramTcThreads)
     __syncthreads();  // H and the windows are rewritten by the next drain
   };
 
-  for (int z = 0; z < g.nz; ++z) {
+  for (int z = zlo; z <= zhi; ++z) {
     if (*abort_flag) break;  // uniform: read after the barrier closing the previous step
-    const int s = z & 1;
-    if (!mbar_wait_bounded(bar_tma(s), (uint32_t)((z >> 1) & 1), status)) *abort_flag = 1;
+    const int it = z - zlo, s = it & 1;
+    if (!mbar_wait_bounded(bar_tma(s), (uint32_t)((it >> 1) & 1), status)) *abort_flag = 1;
     // split plane z into stage s's hi / lo K-major tiles; item (t, 4 voxels) ->
     // one 16-byte core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16. Stage s
     // was last read by plane z-2's MMAs, drained in step z-1.
@@ -257,7 +266,7 @@ __global__ void __launch_bounds__(kGramTcThreads)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();  // tiles written, plane slot s free
     if (tid == kIssuer) {  // a thread of a warp that does not read TMEM back
-      if (z + 2 < g.nz) {
+      if (z + 2 <= zhi) {
         mbar_expect_tx(bar_tma(s), plane_bytes);
         tma_load_4d(planes_addr + (uint32_t)(s * pf * sizeof(float)), &xmap, bar_tma(s), 0, z + 2, cy, cx);
       }
@@ -278,10 +287,10 @@ __global__ void __launch_bounds__(kGramTcThreads)
       }
       umma_commit(bar_mma(s));
     }
-    if (z >= 1) drain(z - 1);  // overlaps plane z's MMAs
+    if (z > zlo) drain(z - 1);  // overlaps plane z's MMAs
     else __syncthreads();
   }
-  if (!*abort_flag && g.nz > 0) drain(g.nz - 1);
+  if (!*abort_flag && zlo <= zhi) drain(zhi);
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kGramTcCols) : "memory");
 }

@@ -77,6 +77,7 @@ struct lrd_plan {
   int gramz_ks = 1;        // voxel-row split per 4x4 Gram block (threads per block)
   size_t smem_gramz;
   int gramz_slots = 0;     // column CTAs resident at once on the device (0: never cut columns)
+  int gramtc_slots = 0;    // the same for the tensor-core column Gram
   int sms = 0;             // multiprocessors of the device
   size_t smem_center, smem_gram, smem_eigh, smem_recon;
   int center_warps;
@@ -348,22 +349,23 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
     const long long cols = P->prob.batch > 0 ? std::max<long long>(1, P->prob.batch / P->g.ncz) : ncol;
     for (long long c0 = col_lo; c0 < col_hi; c0 += cols) {
       const long long nc = std::min(cols, col_hi - c0);
+      // A last wave of a few whole columns would leave most SMs idle while
+      // they finish: cut those columns into window ranges instead.
+      const long long slots = P->use_gramtc ? P->gramtc_slots : P->gramz_slots;
+      long long nfull = nc;
+      int nsplit = 1;
+      const long long rem = slots > 0 ? nc % slots : 0;
+      if (slots > 0 && nc > slots && rem > 0 && 2 * rem <= slots && P->g.ncz > 1) {
+        nsplit = (int)std::min<long long>(P->g.ncz, slots / rem);
+        if (nsplit > 1) nfull = nc - rem;
+        else nsplit = 1;
+      }
+      const long long grid = nfull + (nc - nfull) * nsplit;
       if (P->use_gramtc) {
-        lrd::gram_tc_kernel<<<(unsigned)nc, lrd::kGramTcThreads, P->smem_gramtc, st>>>(map, d_gram + c0 * P->g.ncz * TT, P->g,
-                                                                      P->tab, c0, P->gramz_ring, status);
+        lrd::gram_tc_kernel<<<(unsigned)grid, lrd::kGramTcThreads, P->smem_gramtc, st>>>(
+            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, (int)nfull, nsplit, status);
         rc = launch_check("gram_tc_kernel launch");
       } else {
-        // A last wave of a few whole columns would leave most SMs idle while
-        // they finish: cut those columns into window ranges instead.
-        long long nfull = nc;
-        int nsplit = 1;
-        const long long slots = P->gramz_slots, rem = slots > 0 ? nc % slots : 0;
-        if (slots > 0 && nc > slots && rem > 0 && 2 * rem <= slots && P->g.ncz > 1) {
-          nsplit = (int)std::min<long long>(P->g.ncz, slots / rem);
-          if (nsplit > 1) nfull = nc - rem;
-          else nsplit = 1;
-        }
-        const long long grid = nfull + (nc - nfull) * nsplit;
         lrd::gram_z_kernel<<<(unsigned)grid, lrd::gramz_threads(P->g.nt, P->gramz_ks), P->smem_gramz, st>>>(
             map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, P->gramz_ks, (int)nfull, nsplit,
             status);
@@ -650,6 +652,13 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
         P->gramz_slots = per_sm * sms;
       else
         (void)cudaGetLastError();  // no cut columns; the launches report their own errors
+    }
+    if (!rc && P->use_gramtc) {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lrd::gram_tc_kernel, lrd::kGramTcThreads,
+                                                        P->smem_gramtc) == cudaSuccess)
+        P->gramtc_slots = per_sm * sms;
+      else
+        (void)cudaGetLastError();
     }
   }
   if (!rc) rc = set_smem(eigh_kernel_for(T), P->smem_eigh);

@@ -92,6 +92,21 @@ def test_deterministic_and_batch_invariant(cuda_ok):
     np.testing.assert_array_equal(ra, rc)
 
 
+@pytest.mark.parametrize("form", ["plain", "tensor"])
+@pytest.mark.parametrize("shape", [(96, 96, 48, 48), (48, 48, 24, 48)])
+def test_column_cut_is_bit_identical(cuda_ok, shape, form):
+    """A Gram launch whose last wave holds a few whole patch columns cuts them
+    into window ranges; launches of 100 columns (batch = 100 columns of
+    patches) are never cut. Both give the same output and ranks bit for bit."""
+    from lowrank_gpu_fastest_b200 import make_phantom_lowrank
+    vol = make_phantom_lowrank(shape, seed=5)[0]
+    ncz = len(orc.axis_corners(shape[2], 11, 3))
+    a, ra = run_dev(vol, (11, 11, 11), 3, form=form)
+    b, rb = run_dev(vol, (11, 11, 11), 3, form=form, batch=100 * ncz)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(ra, rb)
+
+
 def test_host_api_matches_device_api(cuda_ok):
     g = load_golden("ref_small")
     vol = golden_input(g)
