@@ -12,9 +12,10 @@
 //    shared memory, which (by symmetry) is column k;
 //  * the reflector vectors are kept in shared memory (HV, one row per step,
 //    zero above the sub-diagonal and 1 on it) and double as the broadcast
-//    buffer of the matrix-vector product;
+//    buffer of the matrix-vector product; row k is stored packed, from its
+//    first live 4-column group (4 * ((k + 1) >> 2)) on, which halves HV;
 //  * inverse iteration keeps its vector and the LU factors in shared memory
-//    (one lane per eigenvector);
+//    and the pivot swaps as bits of a register (one lane per eigenvector);
 //  * the back-transform and the Gram-Schmidt pass work on row-distributed
 //    vectors with warp reductions, 8 vectors at a time.
 //
@@ -39,12 +40,21 @@ __host__ __device__ constexpr int eigh_reg_nr() {
   return (TMAX + 31) / 32;
 }
 
-// Shared-memory floats per warp: HV (TMAX x TMAX), row-k broadcast, w vector,
-// d, e, e2, tau, lam (5 TMAX), LU / MP scratch (4 TMAX kInvGroup), vector
+// Floats of the packed reflector rows: row k (k < n - 2 <= TMAX - 2) holds
+// columns [4 * ((k + 1) >> 2), TMAX).
+template <int TMAX>
+__host__ __device__ constexpr size_t eigh_reg_hv_floats() {
+  size_t f = 0;
+  for (int k = 0; k < TMAX - 2; ++k) f += (size_t)(TMAX - 4 * ((k + 1) >> 2));
+  return f;
+}
+
+// Shared-memory floats per warp: packed HV, row-k broadcast, w vector, d, e,
+// e2, tau, lam (5 TMAX), LU / MP scratch (3 TMAX kInvGroup), vector
 // transpose buffer (TMAX x kLdy).
 template <int TMAX>
 __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
-  return (size_t)TMAX * TMAX + 2 * TMAX + 5 * TMAX + (size_t)4 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
+  return eigh_reg_hv_floats<TMAX>() + 2 * TMAX + 5 * TMAX + (size_t)3 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
 }
 
 // Sturm counts (eigenvalues below x0 and x1) of the tridiagonal held in
@@ -161,16 +171,16 @@ __global__ void __launch_bounds__(32)
                     int* __restrict__ refine_count, int* __restrict__ refine_ids) {
   constexpr int NR = eigh_reg_nr<TMAX>();
   extern __shared__ __align__(16) float sr[];
-  float* HV = sr;                  // TMAX x TMAX reflector vectors
-  float* xk = HV + TMAX * TMAX;    // row k broadcast
+  float* HV = sr;                               // packed reflector vectors
+  float* xk = HV + eigh_reg_hv_floats<TMAX>();  // row k broadcast
   float* ws = xk + TMAX;           // w vector broadcast
   float* d = ws + TMAX;
   float* e = d + TMAX;
   float* e2 = e + TMAX;
   float* tau = e2 + TMAX;
   float* lam = tau + TMAX;
-  float* W = lam + TMAX;                 // LU (4 TMAX kInvGroup) / MP scratch (2 TMAX)
-  float* Yt = W + 4 * TMAX * kInvGroup;  // TMAX x kLdy
+  float* W = lam + TMAX;                 // LU (3 TMAX kInvGroup) / MP scratch (2 TMAX)
+  float* Yt = W + 3 * TMAX * kInvGroup;  // TMAX x kLdy
   const int lane = threadIdx.x;
   const long long b = blockIdx.x;
   const float* G = gram + b * (long long)n * n;
@@ -198,6 +208,7 @@ __global__ void __launch_bounds__(32)
 
   LRD_STAMP(1);
   // ---- Householder tridiagonalisation ---------------------------------------
+  int hbase = 0;  // packed offset of row k of HV
   for (int k = 0; k < n; ++k) {
     // owner of row k broadcasts it (= column k by symmetry)
     if (lane == (k & 31)) {
@@ -244,21 +255,24 @@ __global__ void __launch_bounds__(32)
       e[k] = beta;
       tau[k] = taui;
     }
-    float* hv = HV + k * TMAX;
+    // row k from its first live column group j4lo on; hv[c] = column c
+    const int j4lo = (k + 1) >> 2;
+    float* hv = HV + hbase - 4 * j4lo;
+    hbase += TMAX - 4 * j4lo;
     float vr[NR];
 #pragma unroll
     for (int ri = 0; ri < NR; ++ri) {
       const int r = lane + 32 * ri;
       vr[ri] = (r == k + 1) ? 1.f : ((r >= k + 2 && r < n) ? xr[ri] * sc : 0.f);
-      if (r < TMAX) hv[r] = vr[ri];
+      if (r >= 4 * j4lo && r < TMAX) hv[r] = vr[ri];
     }
     __syncwarp();
     if (taui != 0.f) {
       // p = taui * A22 v over own rows (columns j >= k+1; hv is 0 below).
-      // The column groups j4 < j4lo are dead: a switch on j4lo enters the
-      // unrolled groups at the first live one (cases fall through), so the
-      // register indices stay compile-time and the dead groups cost nothing.
-      const int j4lo = (k + 1) >> 2;
+      // The column groups j4 < j4lo are dead (and not stored): a switch on
+      // j4lo enters the unrolled groups at the first live one (cases fall
+      // through), so the register indices stay compile-time and the dead
+      // groups cost nothing.
       float pr[NR];
 #pragma unroll
       for (int ri = 0; ri < NR; ++ri) {
@@ -343,7 +357,6 @@ __global__ void __launch_bounds__(32)
   float* RU0 = W;
   float* U1 = RU0 + TMAX * kInvGroup;
   float* ML = U1 + TMAX * kInvGroup;
-  float* SW = ML + TMAX * kInvGroup;
   float* V = vecs + b * (long long)n * n;
   for (int j0 = 0; j0 < p; j0 += kInvGroup) {
     const int g = min(kInvGroup, p - j0);
@@ -353,6 +366,7 @@ __global__ void __launch_bounds__(32)
       const float sig = lam[n - 1 - j];
       // LU with partial pivoting of (T - sig I)
       float c = d[0] - sig, s = (n > 1) ? e[0] : 0.f;
+      unsigned long long swb = 0;  // bit i: rows i and i + 1 swapped
       // (the lanes pivot differently: selects, not branches)
       for (int i = 0; i < n - 1; ++i) {
         const float ei = e[i];
@@ -364,7 +378,7 @@ __global__ void __launch_bounds__(32)
         float piv = den;
         U1[i * kInvGroup + q] = keep ? s : an;
         ML[i * kInvGroup + q] = m;
-        SW[i * kInvGroup + q] = keep ? 0.f : 1.f;
+        swb |= (unsigned long long)(!keep) << i;
         const float cn = keep ? fmaf(-m, s, an) : fmaf(-m, an, s);
         s = keep ? en : -m * en;
         c = cn;
@@ -380,7 +394,7 @@ __global__ void __launch_bounds__(32)
         for (int i = 0; i < n - 1; ++i) {
           const float yi = Y[i * kLdy + q], yn = Y[(i + 1) * kLdy + q];
           const float m = ML[i * kInvGroup + q];
-          const bool sw = SW[i * kInvGroup + q] != 0.f;
+          const bool sw = (swb >> i) & 1ull;
           Y[i * kLdy + q] = sw ? yn : yi;
           Y[(i + 1) * kLdy + q] = sw ? fmaf(-m, yn, yi) : fmaf(-m, yi, yn);
         }
@@ -393,7 +407,7 @@ __global__ void __launch_bounds__(32)
           amax = fmaxf(amax, fabsf(x1));
         }
         for (int i = n - 3; i >= 0; --i) {
-          const float u2 = (SW[i * kInvGroup + q] != 0.f) ? e[i + 1] : 0.f;
+          const float u2 = ((swb >> i) & 1ull) ? e[i + 1] : 0.f;
           const float xi = (Y[i * kLdy + q] - U1[i * kInvGroup + q] * x1 - u2 * x2) * RU0[i * kInvGroup + q];
           Y[i * kLdy + q] = xi;
           amax = fmaxf(amax, fabsf(xi));
@@ -426,14 +440,18 @@ __global__ void __launch_bounds__(32)
       for (int q = 0; q < kInvGroup; ++q) yr[ri][q] = (r < n && q < g) ? Yt[r * kLdy + q] : 0.f;
     }
     // back-transform x = H(0) ... H(n-3) y
+    int hb = hbase;  // end of the packed rows
     for (int k = n - 3; k >= 0; --k) {
+      const int j4lo = (k + 1) >> 2;
+      hb -= TMAX - 4 * j4lo;
       const float tk = tau[k];
       if (tk == 0.f) continue;
+      const float* hrow = HV + hb - 4 * j4lo;
       float hr[NR];
 #pragma unroll
       for (int ri = 0; ri < NR; ++ri) {
         const int r = lane + 32 * ri;
-        hr[ri] = (r < n) ? HV[k * TMAX + r] : 0.f;
+        hr[ri] = (r >= 4 * j4lo && r < n) ? hrow[r] : 0.f;
       }
       float dq[kInvGroup];
 #pragma unroll
