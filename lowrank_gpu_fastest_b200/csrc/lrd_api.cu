@@ -334,8 +334,11 @@ int encode_plane_map(const lrd_plan* P, const float* xc, CUtensorMap* map) {
 
 // Gram matrices of the patch columns [col_lo, col_hi) (x-major column index
 // ci * ncy + cj; -1 = all), i.e. of patches [col_lo * ncz, col_hi * ncz).
+// ``spread``: a launch of fewer columns than the device holds at once has all
+// of them cut into window ranges (more, shorter CTAs: lower latency for more
+// plane reads, for a Gram on the critical path of an otherwise idle device).
 int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long long col_lo = 0,
-             long long col_hi = -1) {
+             long long col_hi = -1, bool spread = false) {
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
   const long long ncol = (long long)P->g.ncx * P->g.ncy;
   if (col_hi < 0) col_hi = ncol;
@@ -355,7 +358,11 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
       long long nfull = nc;
       int nsplit = 1;
       const long long rem = slots > 0 ? nc % slots : 0;
-      if (slots > 0 && nc > slots && rem > 0 && 2 * rem <= slots && P->g.ncz > 1) {
+      if (spread && slots > 0 && nc < slots && P->g.ncz > 1) {
+        nsplit = (int)std::min<long long>(P->g.ncz, std::max<long long>(1, slots / nc));
+        if (nsplit > 1) nfull = 0;
+        else nsplit = 1;
+      } else if (slots > 0 && nc > slots && rem > 0 && 2 * rem <= slots && P->g.ncz > 1) {
         nsplit = (int)std::min<long long>(P->g.ncz, slots / rem);
         if (nsplit > 1) nfull = nc - rem;
         else nsplit = 1;
@@ -914,7 +921,7 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
       return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 1), prep));
     planes_in = std::max(planes_in, x_need);
-    if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz))) return rc;
+    if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz, s == 0))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
     LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
     if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false))) return rc;
