@@ -49,12 +49,12 @@ __host__ __device__ constexpr size_t eigh_reg_hv_floats() {
   return f;
 }
 
-// Shared-memory floats per warp: packed HV, row-k broadcast, w vector, d, e,
-// e2, tau, lam (5 TMAX), LU / MP scratch (3 TMAX kInvGroup), vector
-// transpose buffer (TMAX x kLdy).
+// Shared-memory floats per warp: packed HV, d, e, e2, tau, lam (5 TMAX), LU /
+// MP scratch (3 TMAX kInvGroup; during the tridiagonalisation the row-k
+// broadcast and the w vector), vector transpose buffer (TMAX x kLdy).
 template <int TMAX>
 __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
-  return eigh_reg_hv_floats<TMAX>() + 2 * TMAX + 5 * TMAX + (size_t)3 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
+  return eigh_reg_hv_floats<TMAX>() + 5 * TMAX + (size_t)3 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
 }
 
 // Sturm counts (eigenvalues below x0 and x1) of the tridiagonal held in
@@ -171,16 +171,16 @@ __global__ void __launch_bounds__(32)
                     int* __restrict__ refine_count, int* __restrict__ refine_ids) {
   constexpr int NR = eigh_reg_nr<TMAX>();
   extern __shared__ __align__(16) float sr[];
-  float* HV = sr;                               // packed reflector vectors
-  float* xk = HV + eigh_reg_hv_floats<TMAX>();  // row k broadcast
-  float* ws = xk + TMAX;           // w vector broadcast
-  float* d = ws + TMAX;
+  float* HV = sr;  // packed reflector vectors
+  float* d = HV + eigh_reg_hv_floats<TMAX>();
   float* e = d + TMAX;
   float* e2 = e + TMAX;
   float* tau = e2 + TMAX;
   float* lam = tau + TMAX;
   float* W = lam + TMAX;                 // LU (3 TMAX kInvGroup) / MP scratch (2 TMAX)
   float* Yt = W + 3 * TMAX * kInvGroup;  // TMAX x kLdy
+  float* xk = W;                         // tridiagonalisation only: row k broadcast
+  float* ws = W + TMAX;                  //   and the w vector
   const int lane = threadIdx.x;
   const long long b = blockIdx.x;
   const float* G = gram + b * (long long)n * n;
