@@ -437,10 +437,14 @@ def roofline(ph, shape, patch, P, form):
     traffic = ncu_traffic().get(kname)
     if dom in flops_unit:
         achieved = flops_unit[dom] * P / (ph[dom] * 1e-3) / 1e12
+        note = None
+        if not (dom == "gram" and kname == "gram_tc_kernel"):
+            note = ("FFMA on the CUDA cores (float32 products and sums); the fraction is of the bf16 "
+                    "tensor peak, fp32_simt compares the contractions with the measured SGEMM peak")
         return dict(kernel=kname, bound="tensor", achieved=achieved, peak=peaks["bf16_tflops"], unit="TFLOP/s",
                     frac=achieved / peaks["bf16_tflops"], traffic=traffic,
                     peak_source=f"bf16 dense burst {peaks['source']}",
-                    algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch")
+                    algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch", note=note)
     byts = {"center": 2 * vbytes + vbytes // T, "eigh_mp": 2 * P * T * T * 4}[dom]
     achieved = byts / (ph[dom] * 1e-3) / 1e9
     return dict(kernel=kname, bound="hbm", achieved=achieved, peak=peaks["hbm_gbs"], unit="GB/s",
