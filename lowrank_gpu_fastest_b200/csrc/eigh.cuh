@@ -93,6 +93,16 @@ __device__ __forceinline__ float start_entry(int i, int j) {
 }
 
 constexpr int kInvGroup = 8;  // eigenvectors refined concurrently (one lane each)
+
+// Floats of the packed Householder reflector rows of the float32 solvers: row
+// k (k < n - 2 <= TMAX - 2) is stored from its first live 4-column group on,
+// columns [4 * ((k + 1) >> 2), TMAX), about half of TMAX x TMAX.
+template <int TMAX>
+__host__ __device__ constexpr size_t eigh_hv_floats() {
+  size_t f = 0;
+  for (int k = 0; k < TMAX - 2; ++k) f += (size_t)(TMAX - 4 * ((k + 1) >> 2));
+  return f;
+}
 constexpr int kLdy = kInvGroup + 1;  // eigenvector chunk row stride
 constexpr double kRefineTol = 1e-4;  // MP-test margin below which float64 redoes the patch
 

@@ -9,8 +9,9 @@
 //  * Householder: row i of the working matrix in thread i's registers
 //    (a[TMAX], every column index compile-time); at step k the owner of row k
 //    broadcasts it through shared memory (= column k by symmetry); the
-//    reflectors go to shared memory (HV, one row per step) for the
-//    back-transform; the two dot products per step are block reductions;
+//    reflectors go to shared memory (HV, one row per step, stored from its
+//    first live 4-column group on) for the back-transform; the two dot
+//    products per step are block reductions;
 //  * bisection: thread j owns eigenvalue j, after a multisection pass (counts
 //    at TMAX evenly spaced points of the Gerschgorin interval bracket every
 //    eigenvalue at once);
@@ -27,12 +28,13 @@
 
 namespace lrd {
 
-// Shared-memory floats: HV (TMAX x TMAX), row broadcast and w vector (2 TMAX),
-// d, e, e2, tau, lam (5 TMAX), LU / MP scratch / multisection counts (4 TMAX
-// kInvGroup), eigenvector chunk (TMAX x kLdy), reductions (kInvGroup x 4 + 8).
+// Shared-memory floats: packed HV, d, e, e2, tau, lam (5 TMAX), LU / MP
+// scratch / multisection counts (4 TMAX kInvGroup; during the
+// tridiagonalisation the row broadcast and the w vector), eigenvector chunk
+// (TMAX x kLdy), reductions (kInvGroup x 4 + 8).
 template <int TMAX>
 __host__ __device__ constexpr size_t eigh_cta_smem_floats() {
-  return (size_t)TMAX * TMAX + 7 * (size_t)TMAX + (size_t)4 * TMAX * kInvGroup + (size_t)TMAX * kLdy +
+  return eigh_hv_floats<TMAX>() + 5 * (size_t)TMAX + (size_t)4 * TMAX * kInvGroup + (size_t)TMAX * kLdy +
          4 * kInvGroup + 8;
 }
 
@@ -98,10 +100,8 @@ __global__ void __launch_bounds__(TMAX)
                     int* __restrict__ refine_count, int* __restrict__ refine_ids) {
   constexpr int NW = TMAX / 32;
   extern __shared__ __align__(16) float sc[];
-  float* HV = sc;                    // TMAX x TMAX reflector vectors
-  float* xk = HV + TMAX * TMAX;      // row k broadcast
-  float* ws = xk + TMAX;             // w vector broadcast
-  float* d = ws + TMAX;
+  float* HV = sc;  // packed reflector vectors
+  float* d = HV + eigh_hv_floats<TMAX>();
   float* e = d + TMAX;
   float* e2 = e + TMAX;
   float* tau = e2 + TMAX;
@@ -109,6 +109,8 @@ __global__ void __launch_bounds__(TMAX)
   float* W = lam + TMAX;                  // LU (4 TMAX kInvGroup) / MP scratch / counts
   float* Yt = W + 4 * TMAX * kInvGroup;   // TMAX x kLdy
   float* red = Yt + TMAX * kLdy;          // 4 kInvGroup + 8
+  float* xk = W;                          // tridiagonalisation only: row k broadcast
+  float* ws = W + TMAX;                   //   and the w vector
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long long b = blockIdx.x;
   const float* G = gram + b * (long long)n * n;
@@ -128,6 +130,7 @@ __global__ void __launch_bounds__(TMAX)
   LRD_STAMP(1);
 
   // ---- Householder tridiagonalisation -------------------------------------------
+  int hbase = 0;  // packed offset of row k of HV
   for (int k = 0; k < n; ++k) {
     if (tid == k) {
 #pragma unroll
@@ -159,13 +162,15 @@ __global__ void __launch_bounds__(TMAX)
       tau[k] = taui;
     }
     const float vr = (tid == k + 1) ? 1.f : ((tid >= k + 2 && rv) ? xr * scv : 0.f);
-    float* hv = HV + k * TMAX;
-    hv[tid] = vr;
+    // row k from its first live column group j4lo on; hv[c] = column c
+    const int j4lo = (k + 1) >> 2;
+    float* hv = HV + hbase - 4 * j4lo;
+    hbase += TMAX - 4 * j4lo;
+    if (tid >= 4 * j4lo) hv[tid] = vr;
     __syncthreads();
     if (taui != 0.f) {
-      // p = taui * A22 v on the own row; column groups below j4lo are dead (a
-      // switch enters the unrolled groups at the first live one)
-      const int j4lo = (k + 1) >> 2;
+      // p = taui * A22 v on the own row; column groups below j4lo are dead and
+      // not stored (a switch enters the unrolled groups at the first live one)
       float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
 #define LRD_CMV(J)                                                 \
   case J:                                                          \
@@ -361,10 +366,13 @@ __global__ void __launch_bounds__(TMAX)
     for (int q = 0; q < kInvGroup; ++q) yr[q] = (rv && q < g) ? Yt[tid * kLdy + q] : 0.f;
     float* rq = red;  // NW x kInvGroup partial sums
     // back-transform x = H(0) ... H(n-3) y
+    int hb = hbase;  // end of the packed rows
     for (int k = n - 3; k >= 0; --k) {
+      const int j4lo = (k + 1) >> 2;
+      hb -= TMAX - 4 * j4lo;
       const float tk = tau[k];
       if (tk == 0.f) continue;
-      const float hr = rv ? HV[k * TMAX + tid] : 0.f;
+      const float hr = (rv && tid >= 4 * j4lo) ? HV[hb - 4 * j4lo + tid] : 0.f;
       float dq[kInvGroup];
 #pragma unroll
       for (int q = 0; q < kInvGroup; ++q) dq[q] = hr * yr[q];

@@ -40,21 +40,12 @@ __host__ __device__ constexpr int eigh_reg_nr() {
   return (TMAX + 31) / 32;
 }
 
-// Floats of the packed reflector rows: row k (k < n - 2 <= TMAX - 2) holds
-// columns [4 * ((k + 1) >> 2), TMAX).
-template <int TMAX>
-__host__ __device__ constexpr size_t eigh_reg_hv_floats() {
-  size_t f = 0;
-  for (int k = 0; k < TMAX - 2; ++k) f += (size_t)(TMAX - 4 * ((k + 1) >> 2));
-  return f;
-}
-
 // Shared-memory floats per warp: packed HV, d, e, e2, tau, lam (5 TMAX), LU /
 // MP scratch (3 TMAX kInvGroup; during the tridiagonalisation the row-k
 // broadcast and the w vector), vector transpose buffer (TMAX x kLdy).
 template <int TMAX>
 __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
-  return eigh_reg_hv_floats<TMAX>() + 5 * TMAX + (size_t)3 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
+  return eigh_hv_floats<TMAX>() + 5 * TMAX + (size_t)3 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
 }
 
 // Sturm counts (eigenvalues below x0 and x1) of the tridiagonal held in
@@ -172,7 +163,7 @@ __global__ void __launch_bounds__(32)
   constexpr int NR = eigh_reg_nr<TMAX>();
   extern __shared__ __align__(16) float sr[];
   float* HV = sr;  // packed reflector vectors
-  float* d = HV + eigh_reg_hv_floats<TMAX>();
+  float* d = HV + eigh_hv_floats<TMAX>();
   float* e = d + TMAX;
   float* e2 = e + TMAX;
   float* tau = e2 + TMAX;
