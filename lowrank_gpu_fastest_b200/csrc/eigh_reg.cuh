@@ -79,10 +79,12 @@ __device__ __forceinline__ void sturm2_reg(const float (&dr)[TMAX], const float 
 // count(lo) <= j < count(hi), stopped at max(eps tnorm, 2 eps |lambda|): the
 // absolute part is LAPACK's default tolerance (eps times the norm of the
 // tridiagonal), below the float32 reduction's own error in the eigenvalues)
-// with the tridiagonal in registers and one multisection pass first: the 64 chains evaluate counts at 64 evenly spaced
-// interior points of the Gerschgorin interval, and every chain starts from
-// the two neighbouring points that bracket its eigenvalue (six bisection
-// steps for the price of one).
+// with the tridiagonal in registers and one multisection pass first: the 64
+// chains evaluate counts at 64 evenly spaced interior points of the
+// Gerschgorin interval, and every chain starts from the two neighbouring
+// points that bracket its eigenvalue (six bisection steps for the price of
+// one). For TMAX <= 32 each lane owns one eigenvalue and its two chains
+// trisect it.
 template <int TMAX>
 __device__ __forceinline__ void bisect_reg(const float* d, const float* e, const float* e2, float* lam, int n,
                                            float& tnorm_out) {
@@ -126,6 +128,33 @@ __device__ __forceinline__ void bisect_reg(const float* d, const float* e, const
   if (!(lo0 < hi0)) { lo0 = glo; hi0 = ghi; }  // counts not monotone: full interval
   if (!(lo1 < hi1)) { lo1 = glo; hi1 = ghi; }
   const bool has0 = j0 < n, has1 = j1 < n;
+  if constexpr (TMAX <= 32) {
+    // One eigenvalue per lane: the second chain evaluates a second point, so
+    // a step cuts the interval in three (12 instead of 18 steps from the
+    // multisection's interval to the tolerance).
+    bool run = has0;
+    for (int it = 0; it < 200 && run; ++it) {
+      const float tol = fmaxf(abstol, 2.f * eps * fmaxf(fabsf(lo0), fabsf(hi0)));
+      const float w3 = (hi0 - lo0) * (1.f / 3.f);
+      const float ma = lo0 + w3, mb = hi0 - w3;
+      run = hi0 - lo0 > tol && ma > lo0 && ma < mb && mb < hi0;
+      if (!run) break;
+      int ca, cb;
+      sturm2_reg<TMAX>(dr, e2r, ma, mb, pivmin, ca, cb);
+      if (ca > j0) {
+        hi0 = ma;
+      } else if (cb > j0) {
+        lo0 = ma;
+        hi0 = mb;
+      } else {
+        lo0 = mb;
+      }
+    }
+    if (has0) lam[j0] = 0.5f * (lo0 + hi0);
+    __syncwarp();
+    tnorm_out = tnorm;
+    return;
+  }
   bool run0 = has0, run1 = has1;
   for (int it = 0; it < 200 && (run0 || run1); ++it) {
     if (run0) {
