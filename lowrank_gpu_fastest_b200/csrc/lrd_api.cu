@@ -116,7 +116,8 @@ constexpr int kIoSlabsUsed = 10;
 namespace {
 
 // Voxel-row split of the column Gram. Measured on B200 (96x96x48xT, 11^3,
-// stride 3): T = 48 runs 0.80 ms with 2 threads per block (160-thread CTAs)
+// stride 3, before short last waves were cut into window ranges): T = 48
+// runs 0.80 ms with 2 threads per block (160-thread CTAs)
 // against 0.96 ms unsplit and 1.27 ms with 4; T = 32, 64 and 96 are fastest
 // unsplit (0.58 / 1.44 / 1.21 ms, the split costing 30-60%).
 int gramz_split(int T) { return (T > 40 && T <= 56) ? 2 : 1; }
