@@ -128,6 +128,14 @@ int lrd_denoise_host(const lrd_plan* plan, const float* h_vol, float* h_out, int
  * counterpart in the reference (its kernels have no device-side waits). */
 int lrd_workspace_status(const lrd_plan* plan, const void* d_workspace, int32_t* status, void* stream);
 
+/* Self-test of the failure path above, without a GPU fault: a one-thread
+ * kernel waits on a device barrier that nothing completes, gives up after
+ * ``limit_ns`` nanoseconds (1 us .. 10 s) and or-s LRD_STATUS_TMA_TIMEOUT into
+ * the int32 at ``d_status`` (device memory), on ``stream``; the context stays
+ * usable. The kernels' own waits use the same routine with a 2 s limit. No
+ * counterpart in the reference. */
+int lrd_selftest_wait_timeout(int64_t limit_ns, int32_t* d_status, void* stream);
+
 /* Stage entry points, for per-stage parity checks against step 4's unfused
  * route (step4_gram_eigh.py:60-67).
  *   lrd_stage_gram: G = Xc^T Xc for every patch -> d_gram (n_patches, nt, nt).

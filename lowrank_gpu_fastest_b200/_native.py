@@ -56,6 +56,7 @@ SIGNATURES = {
     "lrd_slab_prepare": (ctypes.c_int, [ctypes.c_void_p] * 5),
     "lrd_slab_recon": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "lrd_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
 }
 SLAB_HALO_OUT, SLAB_INTERIOR, SLAB_HALO_IN = 0, 1, 2
 PHASES = ("center", "gram", "eigh_mp", "recon")
@@ -113,6 +114,13 @@ def make_problem(shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, bri
     bx, by, bz = (int(b) for b in (brick or (0, 0, 0)))
     return LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0),
                       bx, by, bz, int(split or 0))
+
+
+def selftest_wait_timeout(limit_ns: int, d_status: int, stream: int):
+    """Run the bounded-wait self-test: a kernel waits on a device barrier that
+    nothing completes and records LRD_STATUS_TMA_TIMEOUT (1) in the int32 at
+    ``d_status`` after ``limit_ns`` ns (asynchronous on ``stream``)."""
+    check(load().lrd_selftest_wait_timeout(int(limit_ns), d_status, stream))
 
 
 def slab_partition(shape, patch, stride, n_slabs):

@@ -50,10 +50,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// Bounded wait for the phase with parity ``parity`` to complete; on expiry
-// ``code`` is or-ed into the status word.
+// Bounded wait for the phase with parity ``parity`` to complete; after
+// ``limit_ns`` ``code`` is or-ed into the status word and the wait gives up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, int* status,
-                                                  int code = kStatusTmaTimeout) {
+                                                  int code = kStatusTmaTimeout,
+                                                  unsigned long long limit_ns = kWaitNs) {
   const unsigned long long t0 = globaltimer_ns();
   for (;;) {
     uint32_t ok;
@@ -63,7 +64,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
         : "r"(bar), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (globaltimer_ns() - t0 > kWaitNs) {
+    if (globaltimer_ns() - t0 > limit_ns) {
       atomicOr(status, code);
       return false;
     }
@@ -224,6 +225,20 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
       }
     }
     __syncthreads();  // this slot is refilled by the TMA issued at the start of the next iteration
+  }
+}
+
+// Self-test of the bounded wait: one thread waits on a freshly initialised
+// mbarrier that nothing arrives at, gives up after ``limit_ns`` and records
+// ``code`` in ``status``; no copy or MMA is in flight, so the kernel simply
+// returns. grid 1, block 32.
+__global__ void wait_timeout_selftest_kernel(int* status, unsigned long long limit_ns, int code) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(&bar);
+    mbar_init(b, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    mbar_wait_bounded(b, 0, status, code, limit_ns);
   }
 }
 

@@ -1085,6 +1085,16 @@ int lrd_workspace_status(const lrd_plan* P, const void* d_ws, int32_t* status, v
   return LRD_OK;
 }
 
+int lrd_selftest_wait_timeout(int64_t limit_ns, int32_t* d_status, void* stream) {
+  g_last_error.clear();
+  if (!d_status) return fail(LRD_ERR_INVALID, "d_status is NULL");
+  if (limit_ns < 1000 || limit_ns > 10000000000ll)
+    return fail(LRD_ERR_INVALID, "limit_ns=%lld not in [1e3, 1e10]", (long long)limit_ns);
+  lrd::wait_timeout_selftest_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+      d_status, (unsigned long long)limit_ns, lrd::kStatusTmaTimeout);
+  return launch_check("wait_timeout_selftest_kernel launch");
+}
+
 int lrd_stage_gram(const lrd_plan* P, const float* d_vol, float* d_gram, void* d_ws, void* stream) {
   int rc = check_plan(P);
   if (rc) return rc;

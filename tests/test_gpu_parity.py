@@ -200,6 +200,28 @@ def test_tensor_core_gram_vs_fp64(cuda_ok, name):
         assert np.abs(gram[idx] - G).max() <= 4e-6 * np.abs(G).max()
 
 
+def test_bounded_wait_gives_up_and_reports(cuda_ok):
+    """The device-wait failure path without a GPU fault: a kernel waits on a
+    barrier that nothing completes, gives up after 20 ms and sets the timeout
+    bit; the context stays usable (a denoise afterwards equals one before)."""
+    import time
+
+    g = load_golden("lowrank_p5s2")
+    vol = golden_input(g)
+    before, rb = run_dev(vol, (5, 5, 5), 2)
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _native.selftest_wait_timeout(20_000_000, st.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    assert int(st.item()) == 1  # LRD_STATUS_TMA_TIMEOUT
+    assert 0.015 <= dt < 5.0
+    after, ra = run_dev(vol, (5, 5, 5), 2)
+    np.testing.assert_array_equal(before, after)
+    np.testing.assert_array_equal(rb, ra)
+
+
 def test_status_word_clear_after_runs(cuda_ok):
     g = load_golden("ref_small")
     vol = torch.from_numpy(golden_input(g)).cuda()

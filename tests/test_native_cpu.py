@@ -71,3 +71,12 @@ def test_valid_problem_without_device_reports_nodevice(lib):
     pr = _native.LrdProblem(48, 48, 24, 48, 11, 11, 11, 3, 0, 0)
     h = ctypes.c_void_p()
     assert lib.lrd_plan_create(ctypes.byref(pr), ctypes.byref(h)) == _native.LRD_ERR_NODEVICE
+
+
+def test_selftest_wait_timeout_checks_arguments(lib):
+    """Bad arguments are rejected on the host, before any device work."""
+    assert lib.lrd_selftest_wait_timeout(10_000_000, None, None) == _native.LRD_ERR_INVALID
+    fake = ctypes.c_void_p(0x1000)  # never dereferenced: the limit check fails first
+    assert lib.lrd_selftest_wait_timeout(10, fake, None) == _native.LRD_ERR_INVALID
+    assert lib.lrd_selftest_wait_timeout(20_000_000_000, fake, None) == _native.LRD_ERR_INVALID
+    assert b"limit_ns" in lib.lrd_last_error_string()
