@@ -15,9 +15,21 @@ rank, with one NCCL halo send/recv between neighbours per step (weak scaling:
 about the single-GPU work per rank); ``--parallel replica`` gives every rank
 an independent volume instead. The step time is the max over ranks.
 
+The headline line also states the accuracy of the timed output (relative L2
+against the reference's step 0 in float32 and float64 on a seeded sample of
+the volume, ranks against both), the ``accurate`` form's times and errors
+(the form at the float64 bar), the reference's own step-8 GPU path timed on
+the same GPU in the same run, and ``torch.linalg.eigh`` on the same Gram
+blocks beside the library's eigensolver phase.
+
 ``--impl reference`` times the reference algorithm's CPU implementation (the
-step-0 NumPy loop restated in oracle/, all host cores through a spawn pool)
-on a bounded sample of the same workload's patches.
+reference's own step-0 NumPy loop from ``baseline/_ref`` when it is
+installed there, else its restatement in oracle/; all host cores through a
+spawn pool) on a bounded sample of the same workload's patches.
+
+``python bench.py --install-reference <checkout>`` installs the reference
+into ``baseline/_ref`` (its pip package, which holds only ``micro/``, plus
+the ladder's top-level modules, unmodified).
 """
 
 from __future__ import annotations
@@ -43,6 +55,83 @@ WORKLOADS = {
                     desc="48x48x24x48 volume, 11^3 patches, stride 3 (1176 patches of 1331x48)"),
 }
 PUBLISHED_STEP8_MS = 66.5  # reference step 8, host->host best of 5, 12600 patches (README.md:48)
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+# golden fixture holding the reference's step-0 output (float32 and float64 runs) on the
+# workload's benchmark phantom with seed 0 and on the ladder's own phantom
+GOLDEN_FOR = {"headline": ("headline_lowrank.npz", "headline_ref.npz"),
+              "config1": ("config1_lowrank.npz", "config1_ref.npz")}
+
+
+def bench_config(wl, world=1):
+    """The ``config`` object both arms print (same keys and values)."""
+    return dict(workload=wl["desc"], shape=list(wl["shape"]), patch=list(wl["patch"]), stride=wl["stride"],
+                phantom="rank-4 [0,1] + N(0,0.05^2), seed 0",
+                l2="flushed by a 256 MiB write between timed GPU steps (outside the events)",
+                parallelism=f"replica x{world}" if world > 1 else "single GPU")
+
+
+def golden_accuracy(out, ranks, fixture):
+    """Errors of a volume ``out`` (numpy, the workload's shape) and per-patch
+    ``ranks`` against a golden fixture of the reference's step 0: relative L2
+    on the fixture's seeded 20000-element sample against the float32 step-0
+    output and the float64 run of the same code, and rank mismatches against
+    both runs' ranks."""
+    import numpy as _np
+
+    d = _np.load(os.path.join(GOLDEN, fixture))
+    idx = d["sample_idx"]
+    o = _np.asarray(out, dtype=_np.float64).reshape(-1)[idx]
+    ref32 = d["out_sample"].astype(_np.float64)
+    ref64 = d["out64_sample"]
+    res = dict(rel_err_vs_fp64=float(_np.linalg.norm(o - ref64) / _np.linalg.norm(ref64)),
+               rel_err_vs_step0=float(_np.linalg.norm(o - ref32) / _np.linalg.norm(ref32)),
+               step0_vs_fp64=float(_np.linalg.norm(ref32 - ref64) / _np.linalg.norm(ref64)),
+               sample=f"{len(idx)}-element seeded sample of the output ({fixture})")
+    if ranks is not None:
+        r = _np.asarray(ranks).astype(_np.int32)
+        res.update(rank_mismatch_vs_step0=int((r != d["ranks"]).sum()),
+                   rank_mismatch_vs_fp64=int((r != d["ranks64"]).sum()), n_patches=int(len(r)))
+    return res
+
+
+def install_reference(src):
+    """Install the reference into ``baseline/_ref``: ``pip install --target``
+    of the reference's package from a copy of the checkout (the package holds
+    only ``micro/``: its pyproject builds no modules), then the ladder's
+    top-level modules (``common.py``, ``stepN_*.py``) copied unmodified beside
+    it, so the ladder's own entry points (and ``micro/``'s ``from common
+    import ...``) import from there."""
+    import shutil
+
+    src = os.path.abspath(src)
+    tmp = tempfile.mkdtemp(prefix="lrd_refsrc_")
+    copy = os.path.join(tmp, "ref")
+    shutil.copytree(src, copy, ignore=shutil.ignore_patterns(".git", "results", "__pycache__"))
+    os.makedirs(REF_DIR, exist_ok=True)
+    cmd = [sys.executable, "-m", "pip", "install", "--no-index", "--no-build-isolation", "--no-deps",
+           "--find-links", "/opt/wheelhouse", "--target", REF_DIR, "--upgrade", copy]
+    rc = subprocess.run(cmd).returncode
+    for f in sorted(os.listdir(src)):
+        if f.endswith(".py"):
+            shutil.copy(os.path.join(src, f), REF_DIR)
+    shutil.rmtree(tmp, ignore_errors=True)
+    print(json.dumps(dict(pip_rc=rc, target=REF_DIR,
+                          modules=sorted(f for f in os.listdir(REF_DIR) if f.endswith(".py")))))
+
+
+def reference_step0():
+    """The reference's own ``step0_numpy_loop`` module from ``baseline/_ref``
+    (None when it is not installed there)."""
+    if not os.path.exists(os.path.join(REF_DIR, "step0_numpy_loop.py")):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    import step0_numpy_loop
+
+    return step0_numpy_loop
+
+
 def phase_kernel(phase, T, form):
     """Kernel that a plan phase launches for T frames (the eigensolve phase
     also runs the refine kernel and its cursor, both under 0.5% of it)."""
@@ -68,6 +157,12 @@ def parse():
     ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (req/s)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-step8", action="store_true", help="skip the reference's step-8 GPU timing")
+    ap.add_argument("--step8-repeats", type=int, default=3, help="step 8: timed host->host calls (best of)")
+    ap.add_argument("--single-form", action="store_true",
+                    help="time only --form (no accurate/plain companion, no ladder-phantom lines)")
+    ap.add_argument("--install-reference", metavar="CHECKOUT", default=None,
+                    help="install the reference checkout into baseline/_ref and exit")
     ap.add_argument("--cpu-sample", type=int, default=0, help="patches in the CPU sample (0 = auto)")
     ap.add_argument("--brick", default=None, help="recon brick bx,by,bz (default: the plan's choice)")
     ap.add_argument("--split", type=int, default=0, help="recon threads per voxel (0 = the plan's choice)")
@@ -84,50 +179,59 @@ def dist_env():
 
 # ----------------------------------------------------------------------------- CPU side
 def cpu_step0_rate(vol, patch, stride, n_patches_sample, processes):
-    """Patches/s of the step-0 loop (oracle port) over a sample of the corner
-    list, spread over ``processes`` spawn workers with one BLAS thread each.
+    """Patches/s of the step-0 loop over a sample of the corner list, spread
+    over ``processes`` spawn workers with one BLAS thread each. The per-patch
+    routine is the reference's own ``step0_numpy_loop.mppca_patch``
+    (step0_numpy_loop.py:8-25) when ``baseline/_ref`` has it, else its
+    restatement in oracle/; returns (rate, seconds, workers, kind).
 
     Each worker receives the volume once (pool initializer) and runs the
     step-0 per-patch work - gather, centre, SVD, MP rank, reconstruct, weighted
-    accumulate into its own ``out``/``wsum`` - over its share of the sample;
-    the wall time of that loop across the pool is the measurement.
+    accumulate into its own ``out``/``wsum`` (step0_numpy_loop.py:32-38) - over
+    its share of the sample; the wall time of that loop across the pool is the
+    measurement.
     """
     import multiprocessing as mp
 
-    from oracle import mppca as orc
+    from lowrank_gpu_fastest_b200.problem import patch_corners
 
-    corners = orc.patch_corners(vol.shape, patch, stride)
+    corners = patch_corners(vol.shape, patch, stride)
     sample = corners[np.linspace(0, len(corners) - 1, n_patches_sample).astype(int)]
     chunks = [c for c in np.array_split(sample, processes) if len(c)]
     for k in ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS"):
         os.environ[k] = "1"
+    use_ref = os.path.exists(os.path.join(REF_DIR, "step0_numpy_loop.py"))
     ctx = mp.get_context("spawn")
-    with ctx.Pool(len(chunks), initializer=_cpu_init, initargs=(vol, patch)) as pool:
+    with ctx.Pool(len(chunks), initializer=_cpu_init, initargs=(vol, patch, use_ref)) as pool:
         pool.map(_cpu_worker, [c[:1] for c in chunks])  # warm (imports, first SVD)
         t0 = time.perf_counter()
         pool.map(_cpu_worker, chunks)
         dt = time.perf_counter() - t0
-    return len(sample) / dt, dt, len(chunks)
+    return len(sample) / dt, dt, len(chunks), ("reference" if use_ref else "port")
 
 
 _CPU = {}
 
 
-def _cpu_init(vol, patch):
+def _cpu_init(vol, patch, use_ref):
     _CPU["vol"] = vol
     _CPU["patch"] = patch
     _CPU["out"] = np.zeros_like(vol)
     _CPU["wsum"] = np.zeros(vol.shape[:3] + (1,), dtype=vol.dtype)
+    if use_ref:
+        _CPU["mppca_patch"] = reference_step0().mppca_patch
+    else:
+        from oracle import mppca as orc
+
+        _CPU["mppca_patch"] = orc.mppca_patch
 
 
 def _cpu_worker(corners):
-    from oracle import mppca as orc
-
     vol, (px, py, pz) = _CPU["vol"], _CPU["patch"]
-    out, wsum = _CPU["out"], _CPU["wsum"]
+    out, wsum, mppca_patch = _CPU["out"], _CPU["wsum"], _CPU["mppca_patch"]
     for i, j, k in corners:
         sl = np.s_[i:i + px, j:j + py, k:k + pz]
-        xd, p = orc.mppca_patch(vol[sl].reshape(-1, vol.shape[-1]))
+        xd, p = mppca_patch(vol[sl].reshape(-1, vol.shape[-1]))
         w = 1.0 / (2.0 + p)
         out[sl] += w * xd.reshape(px, py, pz, -1)
         wsum[sl] += w
@@ -154,23 +258,24 @@ def run_reference(args, wl):
         cpu_step0_rate(vol, wl["patch"], wl["stride"], min(per_step, cores * 4), cores)
     rates = []
     for _ in range(args.steps):
-        r, _, used = cpu_step0_rate(vol, wl["patch"], wl["stride"], per_step, cores)
+        r, _, used, kind = cpu_step0_rate(vol, wl["patch"], wl["stride"], per_step, cores)
         rates.append(r)
     from lowrank_gpu_fastest_b200.problem import n_patches
 
     P = n_patches(wl["shape"], wl["patch"], wl["stride"])
     value = float(statistics.mean(rates))
+    who = ("the reference's own step0_numpy_loop.mppca_patch from baseline/_ref" if kind == "reference"
+           else "the step-0 loop restated in oracle/ (baseline/_ref not installed)")
     line = dict(
         impl="reference", metric="patches_per_s", value=value, unit="patches/s", n_gpus=args.gpus,
         steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * per_step / value,
         ms_per_volume=1e3 * P / value, higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f32", data="synthetic",
-        config=dict(workload=wl["desc"], shape=list(wl["shape"]), patch=list(wl["patch"]),
-                    stride=wl["stride"], phantom="rank-4 [0,1] + N(0,0.05^2), seed 0"),
-        cpu_baseline=dict(value=value, unit="patches/s", cores=used, kind="port",
+        config=bench_config(wl, args.gpus),
+        cpu_baseline=dict(value=value, unit="patches/s", cores=used, kind=kind,
                           sample=f"{per_step} patches per step, evenly spaced over the {P}-patch corner "
-                                 f"list; step-0 NumPy loop (SVD + MP rank + weighted accumulate), one BLAS "
-                                 f"thread per spawn worker"),
+                                 f"list; {who} (SVD + MP rank) with the loop's weighted accumulate, one "
+                                 f"BLAS thread per spawn worker"),
         e2e=dict(value=value, unit="patches/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
     )
     print(json.dumps(line), flush=True)
@@ -273,40 +378,22 @@ def ncu_traffic():
     return {}
 
 
-def run_ours(args, wl):
-    import torch
-    import torch.distributed as dist
-
+def time_form(torch, dist, args, wl, form, vol, rank, world, local, *, clocks=False, golden=None):
+    """Time one form on one resident volume: ``args.steps`` device-timed
+    denoises (CUDA events per step on the launching stream, L2 flushed
+    between steps outside the events; max over ranks), the library's phase
+    events, then the same number of host->host calls through
+    ``lrd_denoise_host`` (pinned host in/out, both copies inside the timed
+    region; max over ranks). With ``golden`` (a fixture name) the output and
+    ranks of the last timed step are checked against it."""
     from lowrank_gpu_fastest_b200 import api
-    from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
 
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
     shape, patch, stride = wl["shape"], wl["patch"], wl["stride"]
-
-    # CPU baseline first (spawn pool before any heavy GPU work), rank 0 at N=1 only
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        vol0, _ = make_phantom_lowrank(shape, seed=0)
-        cores = host_cores()
-        n = args.cpu_sample or max(64, 256 * cores)  # ~10-15 s of CPU work
-        rate, dt, used = cpu_step0_rate(vol0, patch, stride, n, cores)
-        cpu = dict(value=rate, unit="patches/s", cores=used, kind="port",
-                   sample=f"{n} patches evenly spaced over the corner list, step-0 NumPy loop "
-                          f"(SVD + MP rank + weighted accumulate), {used} spawn workers x 1 BLAS "
-                          f"thread, {dt:.1f} s wall")
-
-    vol, _ = make_phantom_lowrank(shape, seed=rank)
     dev = torch.device("cuda", local)
     d_vol = torch.from_numpy(vol).to(dev)
     d_out = torch.empty_like(d_vol)
     brick = tuple(int(v) for v in args.brick.split(",")) if args.brick else None
-    plan = api.get_plan(shape, patch, stride, form=args.form, device=local, brick=brick, split=args.split)
+    plan = api.get_plan(shape, patch, stride, form=form, device=local, brick=brick, split=args.split)
     ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=dev)
     d_ranks = torch.empty(plan.n_patches, dtype=torch.int32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -321,10 +408,11 @@ def run_ours(args, wl):
         flush.zero_()
         step()
     torch.cuda.synchronize()
-
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
+    sampler = None
+    if clocks:
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.3)
     plan.set_profiling(True)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
@@ -341,15 +429,16 @@ def run_ours(args, wl):
     if world > 1:
         dist.barrier()
     wall = time.perf_counter() - t_wall
-    clocks = sampler.stop()
+    clk = sampler.stop() if sampler else None
     phases, ncalls = plan.phase_ms()
     plan.set_profiling(False)
-    ms_total = sum(s.elapsed_time(e) for s, e in evs)
-    t = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    status = plan.status(ws.data_ptr(), sid)
+    t = torch.tensor([sum(s.elapsed_time(e) for s, e in evs)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_per_step = float(t.item()) / args.steps
-    value = world * P / (ms_per_step * 1e-3)
+    out_np = d_out.cpu().numpy()
+    ranks_np = d_ranks.cpu().numpy()
 
     # e2e: host buffers through the C ABI (pinned in/out), copies inside the timed region
     h_in = torch.from_numpy(vol).pin_memory()
@@ -376,57 +465,337 @@ def run_ours(args, wl):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_ms_step = float(t.item())
+    e2e_same = bool(np.array_equal(h_out.numpy(), out_np) and np.array_equal(h_ranks.numpy(), ranks_np))
+    res = dict(form=form, P=P, ms_per_step=ms_per_step, value=world * P / (ms_per_step * 1e-3),
+               e2e_ms=e2e_ms_step, e2e_value=world * P / (e2e_ms_step * 1e-3), wall=wall, clocks=clk,
+               phases={k: v / max(ncalls, 1) for k, v in phases.items()}, status=status,
+               e2e_output_identical=e2e_same, out=out_np, ranks=ranks_np, plan=plan)
+    if golden is not None:
+        res["accuracy"] = golden_accuracy(out_np, ranks_np, golden)
+    del d_vol, d_out, ws, flush, d_in, h_in, h_out
+    return res
+
+
+def library_eigh(torch, wl, vol, local, batch=2048):
+    """``torch.linalg.eigh`` (the eigensolver of the reference's step 8,
+    step8_tuned.py:134) on the same Gram blocks the library's eigensolver
+    phase solves: Grams from ``lrd_stage_gram`` on the resident volume, solved
+    in batches of ``batch`` (step 8's BATCH) and timed with CUDA events, beside
+    ``lrd_stage_eigh`` (eigenvalues, MP ranks, top-p eigenvectors) on the
+    same blocks. The backend is named from the kernels the profiler lists for
+    one batched call."""
+    from lowrank_gpu_fastest_b200 import api
+
+    shape, patch, stride = wl["shape"], wl["patch"], wl["stride"]
+    T = shape[3]
+    dev = torch.device("cuda", local)
+    plan = api.get_plan(shape, patch, stride, form="plain", device=local)
+    P = plan.n_patches
+    d_vol = torch.from_numpy(vol).to(dev)
+    ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=dev)
+    g = torch.empty((P, T, T), dtype=torch.float32, device=dev)
+    sid = torch.cuda.current_stream(dev).cuda_stream
+    plan.stage_gram(d_vol.data_ptr(), g.data_ptr(), ws.data_ptr(), sid)
+    lam = torch.empty((P, T), dtype=torch.float32, device=dev)
+    vecs = torch.empty_like(g)
+    rk = torch.empty(P, dtype=torch.int32, device=dev)
+
+    def ours():
+        plan.stage_eigh(g.data_ptr(), lam.data_ptr(), vecs.data_ptr(), rk.data_ptr(), ws.data_ptr(), sid)
+
+    def lib():
+        for b0 in range(0, P, batch):
+            torch.linalg.eigh(g[b0:b0 + batch])
+
+    def timed(fn, reps):
+        best = 1e30
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e))
+        return best
+
+    torch.linalg.eigh(g[:batch])  # warm (handles, workspaces)
+    ours()
+    torch.cuda.synchronize()
+    res = dict(matrices=P, T=T, batch=batch, ours_ms=timed(ours, 5))
+    res["torch_linalg_eigh_ms"] = timed(lib, 2)
+    res["speedup"] = res["torch_linalg_eigh_ms"] / res["ours_ms"]
+    try:
+        from torch.profiler import ProfilerActivity, profile
+
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            torch.linalg.eigh(g[:256])
+            torch.cuda.synchronize()
+        ks = []
+        for ev in prof.key_averages():
+            tt = getattr(ev, "device_time_total", None)
+            if tt is None:
+                tt = getattr(ev, "cuda_time_total", 0)
+            if tt and tt > 0:
+                ks.append((tt, ev.key))
+        ks.sort(reverse=True)
+        names = [k for _, k in ks[:5]]
+        low = " ".join(names).lower()
+        backend = ("cuSOLVER syevj (Jacobi), batched" if "syevj" in low else
+                   "cuSOLVER syevd" if ("syevd" in low or "stedc" in low or "sytrd" in low) else
+                   "cuSOLVER (kernel names: see eigh_kernels)")
+        res.update(backend=backend, eigh_kernels=names)
+    except Exception as exc:  # the profiler is optional: the timing above stands without it
+        res.update(backend=f"unnamed ({type(exc).__name__}: {exc})")
+    res["torch"] = torch.__version__
+    del g, vecs, ws, d_vol
+    return res
+
+
+def reference_step8(torch, wl, vols, repeats=3, budget_s=60.0):
+    """The reference's step-8 GPU path (``step8_tuned.denoise``,
+    step8_tuned.py:116-146), unmodified, imported from ``baseline/_ref``,
+    on this GPU.
+
+    ``vols``: {name: (volume, golden fixture)}. Per volume: one warm-up call
+    (Triton JIT), then the ladder's own protocol (common.py:129-143: wall
+    clock host->host around the call plus a synchronize, best of up to
+    ``repeats`` calls within ``budget_s``), the device span of one call
+    (CUDA events on the current stream around it: its pageable H2D, the
+    kernels and library calls, the pinned D2H), the call's two copies timed
+    alone the same way, and the device time without them; errors of the
+    output against the golden fixture's step-0 float32 and float64 samples.
+    """
+    if not os.path.exists(os.path.join(REF_DIR, "step8_tuned.py")):
+        return dict(unavailable="baseline/_ref has no step8_tuned.py (python bench.py --install-reference "
+                                "<checkout> installs it)")
+    if tuple(wl["patch"]) != (11, 11, 11):
+        return dict(unavailable="the ladder's patch is fixed at 11^3 (common.py:28)")
+    os.environ["VOL"] = ",".join(str(s) for s in wl["shape"])
+    os.environ["STEP"] = str(wl["stride"])
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    try:
+        import importlib
+
+        import triton
+
+        common = importlib.import_module("common")
+        if tuple(common.VOL_SHAPE) != tuple(wl["shape"]) or common.STEP != wl["stride"]:
+            return dict(unavailable=f"the ladder's common was imported with VOL={common.VOL_SHAPE}, "
+                                    f"STEP={common.STEP}")
+        s8 = importlib.import_module("step8_tuned")
+    except Exception as exc:
+        return dict(unavailable=f"import of the reference's step 8 failed: {type(exc).__name__}: {exc}")
+    res = dict(source="baseline/_ref/step8_tuned.py (unmodified)", torch=torch.__version__,
+               triton=triton.__version__, batch=s8.BATCH, gram_cfg=s8.GRAM_CFG, recon_cfg=s8.RECON_CFG)
+    try:
+        for name, (vol, fixture) in vols.items():
+            t0 = time.perf_counter()
+            out = s8.denoise(vol)
+            torch.cuda.synchronize()
+            first = time.perf_counter() - t0
+            host = []
+            deadline = time.perf_counter() + budget_s
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                out = s8.denoise(vol)
+                torch.cuda.synchronize()
+                host.append(time.perf_counter() - t0)
+                if time.perf_counter() > deadline:
+                    break
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s.record()
+            s8.denoise(vol)
+            e.record()
+            torch.cuda.synchronize()
+            call_ms = s.elapsed_time(e)
+            # the call's copies alone: pageable H2D as torch.from_numpy(vol).cuda() does (step8:118),
+            # D2H into pinned memory as step8:144-146 does
+            s.record()
+            dv = torch.from_numpy(vol).cuda()
+            e.record()
+            torch.cuda.synchronize()
+            h2d = s.elapsed_time(e)
+            hb = torch.empty(dv.shape, pin_memory=True)
+            s.record()
+            hb.copy_(dv)
+            e.record()
+            torch.cuda.synchronize()
+            d2h = s.elapsed_time(e)
+            del dv, hb
+            r = dict(host_ms=1e3 * min(host), host_ms_runs=[1e3 * h for h in host], first_call_ms=1e3 * first,
+                     call_device_ms=call_ms, h2d_ms=h2d, d2h_ms=d2h, device_ms=call_ms - h2d - d2h)
+            if fixture:
+                r["accuracy"] = golden_accuracy(out, None, fixture)
+            res[name] = r
+    except Exception as exc:
+        res["error"] = f"{type(exc).__name__}: {exc}"
+    return res
+
+
+def run_ours(args, wl):
+    import torch
+    import torch.distributed as dist
+
+    from lowrank_gpu_fastest_b200.harness import make_phantom, make_phantom_lowrank
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    shape, patch, stride = wl["shape"], wl["patch"], wl["stride"]
+    wl_name = next((k for k, v in WORKLOADS.items() if v is wl), None)
+    fixtures = GOLDEN_FOR.get(wl_name, (None, None))
+
+    # CPU baseline first (spawn pool before any heavy GPU work), rank 0 at N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        vol0, _ = make_phantom_lowrank(shape, seed=0)
+        cores = host_cores()
+        n = args.cpu_sample or max(64, 256 * cores)  # ~10-15 s of CPU work
+        rate, dt, used, kind = cpu_step0_rate(vol0, patch, stride, n, cores)
+        who = ("the reference's own step0_numpy_loop.mppca_patch (baseline/_ref)" if kind == "reference"
+               else "the step-0 loop restated in oracle/")
+        cpu = dict(value=rate, unit="patches/s", cores=used, kind=kind,
+                   sample=f"{n} patches evenly spaced over the corner list, {who} with the loop's "
+                          f"weighted accumulate, {used} spawn workers x 1 BLAS thread, {dt:.1f} s wall")
+
+    vol, _ = make_phantom_lowrank(shape, seed=rank)
+    golden = fixtures[0] if (rank == 0 and fixtures[0]) else None
+    main = time_form(torch, dist, args, wl, args.form, vol, rank, world, local, clocks=True, golden=golden)
+
+    extra = {}
+    if world == 1 and not args.single_form:
+        # the other forms beside the timed one: accurate meets the float64 bar
+        for f in ("plain", "accurate"):
+            if f != args.form:
+                r = time_form(torch, dist, args, wl, f, vol, rank, world, local, golden=golden)
+                extra[f] = r
+    ladder = {}
+    if world == 1 and fixtures[1] and patch == (11, 11, 11) and not args.single_form:
+        # the ladder's own phantom (common.make_phantom: rank 5 on a ~1000 baseline, sigma 4)
+        vref, _ = make_phantom(shape)
+        for f in ("plain", "accurate"):
+            ladder[f] = time_form(torch, dist, args, wl, f, vref, rank, world, local, golden=fixtures[1])
+    step8, libeigh = None, None
+    if world == 1 and rank == 0 and not args.no_step8 and fixtures[0]:
+        vref = make_phantom(shape)[0] if fixtures[1] else None
+        vols = {"lowrank": (vol, fixtures[0])}
+        if vref is not None:
+            vols["ladder_phantom"] = (vref, fixtures[1])
+        libeigh = library_eigh(torch, wl, vol, local)
+        step8 = reference_step8(torch, wl, vols, repeats=args.step8_repeats)
 
     if rank == 0:
-        ph = {k: v / max(ncalls, 1) for k, v in phases.items()}
-        roof = roofline(ph, shape, patch, P, args.form)
+        P = main["P"]
+        ph = main["phases"]
+        roof = roofline(ph, shape, patch, P, args.form, main["ranks"])
         N = int(np.prod(patch))
         T = shape[3]
         vbytes = int(np.prod(shape)) * 4
         fp32_peak = fp32_simt_peak_tflops(torch)
         tf32_peak = fp32_simt_peak_tflops(torch, tf32=True)
         total_flops = 4 * N * T * T * P
+
+        def summary(r):
+            d = dict(ms_per_volume=r["ms_per_step"], patches_per_s=r["value"], e2e_ms=r["e2e_ms"],
+                     e2e_patches_per_s=r["e2e_value"], phases_ms=r["phases"], device_status=r["status"],
+                     e2e_output_identical=r["e2e_output_identical"])
+            if "accuracy" in r:
+                d["accuracy"] = r["accuracy"]
+            return d
+
         line = dict(
-            metric="patches_per_s", value=value, unit="patches/s", n_gpus=world, steps=args.steps,
-            warmup=args.warmup, ms_per_step=ms_per_step, ms_per_volume=ms_per_step,
+            metric="patches_per_s", value=main["value"], unit="patches/s", n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=main["ms_per_step"], ms_per_volume=main["ms_per_step"],
             higher_is_better=True, scaling="weak",
-            vs_baseline=(world * P / (e2e_ms_step * 1e-3)) / (12600 / (PUBLISHED_STEP8_MS * 1e-3))
-            if wl is WORKLOADS["headline"] else None,
+            vs_baseline=main["e2e_value"] / (12600 / (PUBLISHED_STEP8_MS * 1e-3)) if wl_name == "headline" else None,
             vs_baseline_basis="e2e host->host patches/s / published step-8 (66.5 ms host->host, "
                               "12600 patches, unstated GPU)",
-            dtype="f32", data="synthetic",
-            config=dict(workload=wl["desc"], shape=list(shape), patch=list(patch), stride=stride,
-                        form=args.form, phantom="rank-4 [0,1] + N(0,0.05^2), seed = rank",
-                        l2="flushed by a 256 MiB write between timed steps (outside the events)",
-                        parallelism=f"replica x{world}" if world > 1 else "single GPU"),
-            e2e=dict(value=world * P / (e2e_ms_step * 1e-3), unit="patches/s",
-                     ms_per_step=e2e_ms_step, h2d_bytes_per_step=vbytes,
-                     d2h_bytes_per_step=vbytes + 4 * P,
-                     path="lrd_denoise_host (pinned host in/out, H2D + denoise + D2H + sync)"),
+            dtype="f32", data="synthetic", form=args.form,
+            config=bench_config(wl, world),
+            e2e=dict(value=main["e2e_value"], unit="patches/s", ms_per_step=main["e2e_ms"],
+                     h2d_bytes_per_step=vbytes, d2h_bytes_per_step=vbytes + 4 * P,
+                     path="lrd_denoise_host (pinned host in/out, H2D + denoise + D2H + sync)",
+                     output_identical_to_device_call=main["e2e_output_identical"]),
             phases_ms=ph,
+            device_status=main["status"],
             roofline=roof,
             fp32_simt=dict(peak_tflops_sgemm=fp32_peak, peak_tflops_tf32_gemm=tf32_peak,
-                           achieved_tflops_gram_recon=total_flops / ((ph["gram"] + ph["recon"]) * 1e-3) / 1e12),
+                           algorithmic_tflops_gram_recon=total_flops / ((ph["gram"] + ph["recon"]) * 1e-3) / 1e12,
+                           **executed_fp32(ph, shape, patch, stride, main["ranks"], fp32_peak, args.form)),
             cpu_baseline=cpu,
-            clocks=clocks,
+            clocks=main["clocks"],
             gpu_launches=6 * args.steps,
             gpu_launches_note="per step: center, gram (column TMA or tensor), eigh, eigh_refine, "
                               "refine_advance, recon (plus two status memsets)",
-            wall_s_timed_region=wall,
+            wall_s_timed_region=main["wall"],
         )
+        if "accuracy" in main:
+            line["accuracy"] = main["accuracy"]
+        if extra:
+            line["forms"] = {f: summary(r) for f, r in extra.items()}
+        if ladder:
+            line["ladder_phantom"] = {f: summary(r) for f, r in ladder.items()}
+        if libeigh is not None:
+            line["eigh_vs_library"] = libeigh
+        if step8 is not None:
+            line["reference_step8"] = step8
+            lr = step8.get("lowrank")
+            if lr:
+                allf = dict(extra, **{args.form: main})
+                line["vs_step8"] = {
+                    f"device_{f}": lr["device_ms"] / r["ms_per_step"] for f, r in allf.items()}
+                line["vs_step8"].update({f"e2e_{f}": lr["host_ms"] / r["e2e_ms"] for f, r in allf.items()})
+                line["vs_step8"]["basis"] = ("device: step 8's call on the device less its two copies / our "
+                                             "device-timed denoise; e2e: step 8 host->host best-of / our "
+                                             "lrd_denoise_host; both on the benchmark phantom")
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def roofline(ph, shape, patch, P, form):
+def executed_fp32(ph, shape, patch, stride, ranks, fp32_peak, form):
+    """FP32 work the Gram and reconstruction kernels execute (not the 2 N T^2
+    per patch of the full-square algorithmic count), over their phase times,
+    as a fraction of the measured SGEMM rate: the column Gram forms each
+    z-plane's Gram once per (x, y) column on the upper triangle in 4x4 blocks
+    and adds it into the windows; the reconstruction does y = (x - m) V_p^T
+    and y V_p (4 p T flops) for every covered voxel-patch pair."""
+    from lowrank_gpu_fastest_b200.problem import axis_corners
+
+    X, Y, Z, T = shape
+    px, py, pz = patch
+    ncx = len(axis_corners(X, px, stride))
+    ncy = len(axis_corners(Y, py, stride))
+    nb = (T + 3) // 4
+    gram_fl = 2.0 * ncx * ncy * Z * px * py * 16 * nb * (nb + 1) / 2
+    N = px * py * pz
+    recon_fl = float(4 * T * N * np.asarray(ranks, dtype=np.float64).sum())
+    out = dict(executed_gflop_gram=gram_fl / 1e9, executed_gflop_recon=recon_fl / 1e9,
+               mean_rank=float(np.mean(ranks)))
+    if form != "tensor" or T > 64:
+        out["executed_tflops_gram"] = gram_fl / (ph["gram"] * 1e-3) / 1e12
+        out["gram_frac_of_sgemm"] = out["executed_tflops_gram"] / fp32_peak
+    out["executed_tflops_recon"] = recon_fl / (ph["recon"] * 1e-3) / 1e12
+    out["recon_frac_of_sgemm"] = out["executed_tflops_recon"] / fp32_peak
+    return out
+
+
+def roofline(ph, shape, patch, P, form, ranks=None):
     """``roofline`` object for the dominant phase of one denoise (phase ms
     ``ph``): algorithmic FLOPs (Gram, reconstruction: 2 N T^2 per patch) or
     bytes (centre: volume in/out + means; eigensolve: Gram block in and
     eigenvector block out, 2 T^2 x 4 per patch) per launch over the phase's
     event time, against the measured peaks; DRAM traffic per launch from the
-    committed ncu summary."""
+    committed ncu summary. For the reconstruction the executed FP32 rate
+    (4 p T flops per covered voxel-patch pair, p the patch's rank) is given
+    beside it."""
     peaks = measured_peaks()
     dom = max(ph, key=ph.get)
     N = int(np.prod(patch))
@@ -440,11 +809,16 @@ def roofline(ph, shape, patch, P, form):
         note = None
         if not (dom == "gram" and kname == "gram_tc_kernel"):
             note = ("FFMA on the CUDA cores (float32 products and sums); the fraction is of the bf16 "
-                    "tensor peak, fp32_simt compares the contractions with the measured SGEMM peak")
-        return dict(kernel=kname, bound="tensor", achieved=achieved, peak=peaks["bf16_tflops"], unit="TFLOP/s",
-                    frac=achieved / peaks["bf16_tflops"], traffic=traffic,
-                    peak_source=f"bf16 dense burst {peaks['source']}",
-                    algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch", note=note)
+                    "tensor peak, fp32_simt compares the executed work with the measured SGEMM peak")
+        r = dict(kernel=kname, bound="tensor", achieved=achieved, peak=peaks["bf16_tflops"], unit="TFLOP/s",
+                 frac=achieved / peaks["bf16_tflops"], traffic=traffic,
+                 peak_source=f"bf16 dense burst {peaks['source']}",
+                 algorithmic=f"2*N*T^2 = {flops_unit[dom]} flop/patch x {P} patches per launch", note=note)
+        if dom == "recon" and ranks is not None:
+            ex = 4.0 * T * N * float(np.asarray(ranks, dtype=np.float64).sum())
+            r["executed_tflops"] = ex / (ph[dom] * 1e-3) / 1e12
+            r["executed"] = "4*p*T flop per covered voxel-patch pair (rank-p projection)"
+        return r
     byts = {"center": 2 * vbytes + vbytes // T, "eigh_mp": 2 * P * T * T * 4}[dom]
     achieved = byts / (ph[dom] * 1e-3) / 1e9
     return dict(kernel=kname, bound="hbm", achieved=achieved, peak=peaks["hbm_gbs"], unit="GB/s",
@@ -679,6 +1053,8 @@ def run_serving(args):
 
 def main():
     args = parse()
+    if args.install_reference:
+        return install_reference(args.install_reference)
     if args.workload == "batched":
         return run_batched(args)
     if args.workload == "serving":

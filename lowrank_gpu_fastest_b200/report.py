@@ -10,6 +10,13 @@ on nsys captures. Here the sources are the plan's own CUDA-event phase ring
     python -m lowrank_gpu_fastest_b200.report target [--shape ...] [--form ...] [--reps 2]
     python -m lowrank_gpu_fastest_b200.report ncu-table launches.csv [--skip REGEX]
     python -m lowrank_gpu_fastest_b200.report summary bench1.json [bench2.json ...]
+    python -m lowrank_gpu_fastest_b200.report rank-agreement case1.npz [case2.npz ...] [--forms plain,accurate]
+    python -m lowrank_gpu_fastest_b200.report harness [--shape ...] [--form ...] [--phantom ladder|lowrank]
+                                                      [--ref step0_out.npy] [--json out.json]
+
+``harness`` times the library's host->host ``denoise`` the way the ladder's
+``common.run`` (common.py:103-172) times a rung: warm-up call, best of up to
+5 calls within 60 s, relative L2 against a saved step-0 output when given.
 
 ``target`` is the workload for an ncu capture: it denoises the synthetic
 volume ``reps`` times (device-resident) and exits.
@@ -141,6 +148,76 @@ def summary(lines):
                            "SM MHz"], rows)
 
 
+def regenerate_input(rec):
+    """Input volume of a case record (``gen``: "ref" = the ladder's phantom,
+    "lowrank" = the benchmark phantom, "const" = a constant 3.0 volume;
+    ``shape``; ``gen_kwargs`` as a Python literal)."""
+    import ast
+
+    import numpy as np
+
+    from .harness import make_phantom, make_phantom_lowrank
+
+    shape = tuple(int(s) for s in rec["shape"])
+    kw = ast.literal_eval(str(rec["gen_kwargs"]))
+    gen = str(rec["gen"])
+    if gen == "ref":
+        return make_phantom(shape, **kw)[0]
+    if gen == "lowrank":
+        return make_phantom_lowrank(shape, **kw)[0]
+    if gen == "const":
+        return np.full(shape, 3.0, dtype=np.float32)
+    raise ValueError(f"unknown generator {gen!r}")
+
+
+def count_mismatches(ranks, ranks32, ranks64):
+    """MP-rank disagreements of ``ranks`` with a float32 and a float64 run of
+    the step-0 loop, and of those two runs with each other."""
+    import numpy as np
+
+    r, a, b = (np.asarray(v).astype(np.int64) for v in (ranks, ranks32, ranks64))
+    return dict(n=int(len(r)), vs_step0=int((r != a).sum()), vs_fp64=int((r != b).sum()),
+                step0_vs_fp64=int((a != b).sum()))
+
+
+def rank_agreement(paths, forms=("plain", "accurate", "tensor")):
+    """Rank agreement in the manner of the ladder's micro/rank_agreement.py:
+    46-102 (which counts the MP-rank mismatches of FP32 routes against an FP64
+    SVD): for every case file (an ``.npz`` with the input's generator, shape,
+    patch, stride and the per-patch ranks of step 0 run in float32,
+    ``ranks``, and in float64, ``ranks64``) and every form, the library's
+    ranks (device-resident call) against both. Returns a list of rows."""
+    import os
+
+    import numpy as np
+    import torch
+
+    from . import api
+
+    rows = []
+    for path in paths:
+        d = np.load(path)
+        vol = regenerate_input(d)
+        patch, stride = tuple(int(v) for v in d["patch"]), int(d["stride"])
+        dv = torch.from_numpy(vol).cuda()
+        for form in forms:
+            _, rk = api.denoise(dv, patch, stride, form=form, return_ranks=True)
+            rk = rk.cpu().numpy()
+            rows.append(dict(case=os.path.basename(path).rsplit(".", 1)[0], shape=tuple(vol.shape),
+                             patch=patch, stride=stride, form=form,
+                             **count_mismatches(rk, d["ranks"], d["ranks64"])))
+        del dv
+    return rows
+
+
+def rank_table(rows):
+    return markdown_table(["case", "shape", "patch / stride", "form", "patches", "vs step 0 (fp32)",
+                           "vs fp64", "step 0 vs fp64"],
+                          [[r["case"], "x".join(map(str, r["shape"])), f"{r['patch'][0]}^3 / {r['stride']}"
+                            if len(set(r["patch"])) == 1 else f"{r['patch']} / {r['stride']}", r["form"], r["n"],
+                            r["vs_step0"], r["vs_fp64"], r["step0_vs_fp64"]] for r in rows])
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m lowrank_gpu_fastest_b200.report")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -156,6 +233,18 @@ def main(argv=None):
     p.add_argument("--skip", default=None)
     p = sub.add_parser("summary")
     p.add_argument("files", nargs="+")
+    p = sub.add_parser("harness")
+    p.add_argument("--shape", type=_shape, default=(96, 96, 48, 48))
+    p.add_argument("--patch", type=_shape, default=(11, 11, 11))
+    p.add_argument("--stride", type=int, default=3)
+    p.add_argument("--form", default="plain")
+    p.add_argument("--phantom", choices=["ladder", "lowrank"], default="ladder")
+    p.add_argument("--repeats", type=int, default=5)
+    p.add_argument("--ref", default=None, help=".npy of the step-0 output on the same phantom")
+    p.add_argument("--json", default=None)
+    p = sub.add_parser("rank-agreement")
+    p.add_argument("cases", nargs="+")
+    p.add_argument("--forms", default="plain,accurate,tensor")
     a = ap.parse_args(argv)
     if a.cmd == "breakdown":
         r = phase_breakdown(a.shape, a.patch, a.stride, a.form, a.reps)
@@ -183,6 +272,29 @@ def main(argv=None):
         print(markdown_table(["kernel", "launches", "total ms", "mean us", "share"],
                              [[r["kernel"], r["launches"], f"{r['total_ms']:.3f}", f"{r['mean_us']:.1f}",
                                f"{100 * r['share']:.1f}%"] for r in t]))
+    elif a.cmd == "harness":
+        import functools
+
+        import numpy as np
+        import torch
+
+        from . import api
+        from .harness import make_phantom, make_phantom_lowrank, run
+        from .problem import n_patches
+
+        gen = make_phantom if a.phantom == "ladder" else make_phantom_lowrank
+        noisy, clean = gen(a.shape)
+        ref = np.load(a.ref) if a.ref else None
+        fn = functools.partial(api.denoise, patch=a.patch, stride=a.stride, form=a.form)
+        res, _ = run(f"lrd_{a.form}", fn, noisy, clean, ref, n_patches(a.shape, a.patch, a.stride),
+                     repeats=a.repeats, sync=torch.cuda.synchronize, out_json=a.json)
+        print(f"[{res['name']}] volume {tuple(a.shape)}, patch {tuple(a.patch)}, stride {a.stride}, "
+              f"{res['n_patches']} patches")
+        print(f"  best {res['seconds'] * 1e3:9.2f} ms   ({res['us_per_patch']:8.3f} us/patch)   "
+              f"first call {res['first_call'] * 1e3:.0f} ms")
+        print(json.dumps(res))
+    elif a.cmd == "rank-agreement":
+        print(rank_table(rank_agreement(a.cases, tuple(a.forms.split(",")))))
     elif a.cmd == "summary":
         lines = []
         for f in a.files:

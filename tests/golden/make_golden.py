@@ -1,9 +1,9 @@
 """Regenerate the golden fixtures from the reference ladder's own step-0 loop.
 
-Run in a container that has the reference checkout (read-only) at
-``/root/reference``:
+Run where a checkout of the reference exists (it is only read), giving its
+path as an argument or in ``LRD_REFERENCE``:
 
-    python tests/golden/make_golden.py [--skip-large]
+    python tests/golden/make_golden.py --reference <checkout> [--skip-large]
 
 The reference's ``common.py`` writes a ``results/`` folder next to itself on
 import, so the script copies the reference's Python files into a temporary
@@ -38,8 +38,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
 
 from lowrank_gpu_fastest_b200.harness import make_phantom, make_phantom_lowrank  # noqa: E402
-
-REFERENCE = "/root/reference"
 
 SMALL = [
     # name, generator, shape, patch, stride, gen kwargs
@@ -76,10 +74,10 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def load_reference(tmp):
-    for f in os.listdir(REFERENCE):
+def load_reference(tmp, reference):
+    for f in os.listdir(reference):
         if f.endswith(".py"):
-            shutil.copy(os.path.join(REFERENCE, f), tmp)
+            shutil.copy(os.path.join(reference, f), tmp)
     sys.path.insert(0, tmp)
     common = importlib.import_module("common")
     s0 = importlib.import_module("step0_numpy_loop")
@@ -108,9 +106,13 @@ def run_step0(common, s0, vol, patch, stride):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-large", action="store_true")
+    ap.add_argument("--reference", default=os.environ.get("LRD_REFERENCE"),
+                    help="path of the reference checkout (default: $LRD_REFERENCE)")
     args = ap.parse_args()
+    if not args.reference or not os.path.isdir(args.reference):
+        ap.error("give the reference checkout with --reference or LRD_REFERENCE")
     tmp = tempfile.mkdtemp(prefix="lrd_ref_")
-    common, s0 = load_reference(tmp)
+    common, s0 = load_reference(tmp, args.reference)
     # the package's phantom must reproduce the ladder's bit for bit
     for shape in [(17, 15, 13, 24), (12, 11, 10, 16)]:
         a = common.make_phantom(shape)[0]

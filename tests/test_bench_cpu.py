@@ -44,3 +44,42 @@ def test_contract_arguments(monkeypatch):
     assert (a.gpus, a.steps, a.warmup, a.impl, a.parallel) == (2, 3, 4, "ours", "shard")
     monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference"])
     assert bench.parse().impl == "reference"
+
+
+def test_golden_accuracy_of_the_step0_sample():
+    """The accuracy block of the bench line: the step-0 sample itself has zero
+    error against step 0, its own distance from float64, and no rank
+    mismatches with step 0."""
+    import numpy as np
+
+    d = np.load(os.path.join(ROOT, "tests", "golden", "config1_lowrank.npz"))
+    out = np.zeros(tuple(int(s) for s in d["shape"]), dtype=np.float32)
+    out.reshape(-1)[d["sample_idx"]] = d["out_sample"]
+    a = bench.golden_accuracy(out, d["ranks"], "config1_lowrank.npz")
+    assert a["rel_err_vs_step0"] == 0.0
+    assert a["rel_err_vs_fp64"] == pytest.approx(a["step0_vs_fp64"])
+    assert 1e-8 < a["rel_err_vs_fp64"] < 1e-6
+    assert a["rank_mismatch_vs_step0"] == 0 and a["n_patches"] == 1176
+
+
+def test_executed_fp32_counts():
+    """Executed FP32 work: the column Gram's plane Grams (upper-triangle 4x4
+    blocks, one per plane per (x, y) column) and the reconstruction's 4 p T
+    flops per covered voxel-patch pair."""
+    import numpy as np
+
+    ranks = np.full(12600, 4, dtype=np.int32)
+    ph = {"center": 0.05, "gram": 0.68, "eigh_mp": 1.1, "recon": 1.2}
+    r = bench.executed_fp32(ph, (96, 96, 48, 48), (11, 11, 11), 3, ranks, 64.0, "plain")
+    assert r["executed_gflop_gram"] == pytest.approx(2 * 30 * 30 * 48 * 121 * 16 * 78 / 1e9)
+    assert r["executed_gflop_recon"] == pytest.approx(4 * 48 * 1331 * 4 * 12600 / 1e9)
+    assert r["recon_frac_of_sgemm"] == pytest.approx(r["executed_tflops_recon"] / 64.0)
+
+
+def test_rank_mismatch_counts():
+    from lowrank_gpu_fastest_b200 import report
+
+    r = report.count_mismatches([1, 2, 3, 4], [1, 2, 3, 5], [1, 0, 3, 5])
+    assert r == dict(n=4, vs_step0=1, vs_fp64=2, step0_vs_fp64=1)
+    assert "vs fp64" in report.rank_table([dict(case="c", shape=(4, 4, 4, 8), patch=(3, 3, 3), stride=1,
+                                                form="plain", **r)])
