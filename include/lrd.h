@@ -14,8 +14,15 @@
  *     lrd_last_error_string() gives a message for the calling thread's last
  *     failure;
  *   - a volume is float32, C order (x, y, z, t), t contiguous;
- *   - a plan is immutable after creation and may be shared between threads;
- *     one stream must not run two calls on the same workspace at once.
+ *   - a plan's problem, tables and launch shapes do not change after creation,
+ *     and lrd_denoise, the stage entry points and lrd_noise_map may be called
+ *     on one plan from several threads at once (each call on its own
+ *     workspace) while its profiling is off. Two parts of a plan are mutable:
+ *     with profiling on (lrd_plan_set_profiling) every lrd_denoise records
+ *     into the plan's event ring, so profiled calls must come from one thread;
+ *     lrd_denoise_host drives the plan's own copy and compute streams and
+ *     events, so it runs one call at a time per plan. One stream must not run
+ *     two calls on the same workspace at once.
  */
 #ifndef LRD_H
 #define LRD_H
@@ -174,6 +181,13 @@ int lrd_plan_phase_ms(lrd_plan* plan, float* ms /* LRD_NUM_PHASES */, int32_t* n
  * 21 MiB for a 48x48x24x48 volume with 11^3 patches at stride 3; the
  * 96x96x48x48 headline needs about 203 MiB) are rejected with
  * LRD_ERR_UNSUPPORTED and a message giving the size needed.
+ *
+ * The problem's fields mean what they mean for lrd_plan_create (brick and
+ * recon_split included); d_vol and d_out must not overlap. Every form runs
+ * its Gram on the per-patch FP32 kernel here (the tensor form's tcgen05 Gram
+ * and the column Gram are not used), so the tensor form gives the accurate
+ * form's result; the patch-index tables are written into the array by a
+ * kernel on ``stream``.
  *
  * The first call on a device looks up the array's device address (with that
  * device current) and caches it; make that first call before any stream

@@ -22,8 +22,11 @@
 // 32w..32w+15 of warp w's sub-partition) and added in float32 into the
 // windows' rows in shared memory; a completed window is written out.
 //
-// Waits (TMA and MMA completion) are bounded by %globaltimer deadlines; the
-// TMEM allocation is released on every path.
+// Waits (TMA and MMA completion) are bounded by %globaltimer deadlines. When
+// one gives up, the CTA issues no further copy or MMA, the issuing thread
+// waits (with the same bound) for the copies and MMAs it still has in flight,
+// and only then is the TMEM allocation released and the CTA retired; the
+// status word records the timeout.
 #pragma once
 
 #include "gram_z.cuh"
@@ -180,10 +183,18 @@ __global__ void __launch_bounds__(kGramTcThreads)
   auto bar_tma = [&](int s) { return (uint32_t)__cvta_generic_to_shared(&bars[s]); };
   auto bar_mma = [&](int s) { return (uint32_t)__cvta_generic_to_shared(&bars[2 + s]); };
 
+  // Work the issuing thread has in flight: per plane slot / accumulator, whether
+  // a phase of its barrier is pending and that phase's parity. Each barrier has
+  // at most one phase pending: a slot (accumulator) is refilled only after every
+  // thread's wait for its previous plane succeeded (nothing is issued once a
+  // wait has given up).
+  bool tma_pend[2] = {false, false}, mma_pend[2] = {false, false};
+  uint32_t tma_par[2] = {0, 0}, mma_par[2] = {0, 0};
   if (tid == kIssuer) {
     for (int i = 0; i < 2 && zlo + i <= zhi; ++i) {
       mbar_expect_tx(bar_tma(i), plane_bytes);
       tma_load_4d(planes_addr + (uint32_t)(i * pf * sizeof(float)), &xmap, bar_tma(i), 0, zlo + i, cy, cx);
+      tma_pend[i] = true;
     }
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
@@ -194,6 +205,8 @@ __global__ void __launch_bounds__(kGramTcThreads)
     const int s = (zr - zlo) & 1;
     if (!mbar_wait_bounded(bar_mma(s), (uint32_t)(((zr - zlo) >> 1) & 1), status, kStatusMmaTimeout))
       *abort_flag = 1;
+    else if (tid == kIssuer)
+      mma_pend[s] = false;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (warp < 4 && warp * 16 < T) {  // M = 64: rows 16w..16w+15 in lanes 0..15 of sub-partition w
       const int trow = warp * 16 + lane;
@@ -242,7 +255,10 @@ __global__ void __launch_bounds__(kGramTcThreads)
   for (int z = zlo; z <= zhi; ++z) {
     if (*abort_flag) break;  // uniform: read after the barrier closing the previous step
     const int it = z - zlo, s = it & 1;
-    if (!mbar_wait_bounded(bar_tma(s), (uint32_t)((it >> 1) & 1), status)) *abort_flag = 1;
+    if (!mbar_wait_bounded(bar_tma(s), (uint32_t)((it >> 1) & 1), status))
+      *abort_flag = 1;
+    else if (tid == kIssuer)
+      tma_pend[s] = false;
     // split plane z into stage s's hi / lo K-major tiles; item (t, 4 voxels) ->
     // one 16-byte core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16. Stage s
     // was last read by plane z-2's MMAs, drained in step z-1.
@@ -265,10 +281,12 @@ __global__ void __launch_bounds__(kGramTcThreads)
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();  // tiles written, plane slot s free
-    if (tid == kIssuer) {  // a thread of a warp that does not read TMEM back
+    if (tid == kIssuer && !*abort_flag) {  // a thread of a warp that does not read TMEM back
       if (z + 2 <= zhi) {
         mbar_expect_tx(bar_tma(s), plane_bytes);
         tma_load_4d(planes_addr + (uint32_t)(s * pf * sizeof(float)), &xmap, bar_tma(s), 0, z + 2, cy, cx);
+        tma_pend[s] = true;
+        tma_par[s] = (uint32_t)(((it + 2) >> 1) & 1);
       }
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const uint32_t hi_addr = smt_addr + (uint32_t)(s * 2 * tile), lo_addr = hi_addr + (uint32_t)tile;
@@ -286,12 +304,25 @@ __global__ void __launch_bounds__(kGramTcThreads)
         dl += 16;
       }
       umma_commit(bar_mma(s));
+      mma_pend[s] = true;
+      mma_par[s] = (uint32_t)((it >> 1) & 1);
     }
     if (z > zlo) drain(z - 1);  // overlaps plane z's MMAs
     else __syncthreads();
   }
   if (!*abort_flag && zlo <= zhi) drain(zhi);
   __syncthreads();
+  if (*abort_flag && tid == kIssuer) {
+    // a wait gave up: let the copies and MMAs still in flight land (bounded)
+    // before the tensor memory and the shared memory they write are released
+    for (int i = 0; i < 2; ++i) {
+      if (tma_pend[i]) mbar_wait_bounded(bar_tma(i), tma_par[i], status);
+      if (mma_pend[i]) mbar_wait_bounded(bar_mma(i), mma_par[i], status, kStatusMmaTimeout);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kGramTcCols) : "memory");
 }
 

@@ -22,9 +22,11 @@
 // The K = px*py*pz sum therefore rounds as a two-level blocked sum, plane then
 // window (the per-patch kernel rounds as x-plane then float64 window).
 //
-// Every mbarrier wait is bounded by a %globaltimer deadline; on expiry the
-// kernel records LRD_STATUS_TMA_TIMEOUT in the status word and carries on
-// (the result is then invalid and the host reports it).
+// Every mbarrier wait is bounded by a %globaltimer deadline. On expiry the
+// kernel records LRD_STATUS_TMA_TIMEOUT in the status word (the result is
+// then invalid and the host reports it), issues no further copy, and the
+// issuing thread waits - with the same bound - for the copies it still has in
+// flight into the CTA's shared memory before the CTA exits.
 #pragma once
 
 #include <cuda.h>
@@ -78,6 +80,15 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map
       "%5}], [%6];\n" ::"r"(dst),
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
       : "memory");
+}
+
+// After a wait gave up: wait (bounded) for the copies still in flight into the
+// CTA's shared memory - the one whose wait gave up (``a``) and the one issued
+// after it (``b``) - before the CTA exits.
+__device__ __noinline__ void drain_copies(bool wait_a, uint32_t bar_a, uint32_t par_a, bool wait_b,
+                                          uint32_t bar_b, uint32_t par_b, int* status) {
+  if (wait_a) mbar_wait_bounded(bar_a, par_a, status);
+  if (wait_b) mbar_wait_bounded(bar_b, par_b, status);
 }
 
 __host__ __device__ inline size_t gramz_plane_floats(int rows, int T) {
@@ -160,15 +171,21 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
     tma_load_4d((uint32_t)__cvta_generic_to_shared(plane0), &xmap, bar0, 0, zlo, cy, cx);
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
-  for (int z = zlo; z <= zhi; ++z) {
+  int gave_up = 0;  // uniform: a wait of some thread gave up at plane stop_z
+  int stop_z = zhi;
+  bool own_wait_ok = true;
+  for (int z = zlo; z <= zhi && !gave_up; ++z) {
     const int it = z - zlo, slot = it & 1;
-    if (tid == 0 && z + 1 <= zhi) {
+    // Each slot's barrier has at most one phase pending: plane z + 1 goes into
+    // the slot whose previous plane (z - 1) every thread waited for in full.
+    const bool issued_next = z + 1 <= zhi;
+    if (tid == 0 && issued_next) {
       const uint32_t nb_ = slot ? bar0 : bar1;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       mbar_expect_tx(nb_, plane_bytes);
       tma_load_4d((uint32_t)__cvta_generic_to_shared(slot ? plane0 : plane1), &xmap, nb_, 0, z + 1, cy, cx);
     }
-    mbar_wait_bounded(slot ? bar1 : bar0, (uint32_t)((it >> 1) & 1), status);
+    const bool ok = mbar_wait_bounded(slot ? bar1 : bar0, (uint32_t)((it >> 1) & 1), status);
     const int klo = max(tab.cover[2][2 * z], wlo), khi = min(tab.cover[2][2 * z + 1], whi);
     if (klo <= khi) {
       const float* pl = slot ? plane1 : plane0;
@@ -224,7 +241,18 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
         }
       }
     }
-    __syncthreads();  // this slot is refilled by the TMA issued at the start of the next iteration
+    // this slot is refilled by the TMA issued at the start of the next iteration
+    gave_up = __syncthreads_or(!ok);
+    stop_z = z;
+    own_wait_ok = ok;
+  }
+  if (gave_up && tid == 0) {
+    // a wait gave up: nothing more was issued; wait (bounded) for the copies
+    // still in flight - plane stop_z if this thread's own wait gave up, and
+    // plane stop_z + 1 - so that none lands after the CTA's shared memory is freed
+    const int it = stop_z - zlo, slot = it & 1;
+    drain_copies(!own_wait_ok, slot ? bar1 : bar0, (uint32_t)((it >> 1) & 1), stop_z + 1 <= zhi,
+                 slot ? bar0 : bar1, (uint32_t)(((it + 1) >> 1) & 1), status);
   }
 }
 

@@ -484,13 +484,8 @@ int check_plan(const lrd_plan* P) {
   return LRD_OK;
 }
 
-// Plan for ``pr``; ``x_corners`` (nullable) replaces the x-axis corner list
-// (a slab of a larger volume), which must be sorted, start >= 0 and end
-// with a patch inside the volume.
-int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lrd_plan** out) {
-  g_last_error.clear();
-  if (!pr || !out) return fail(LRD_ERR_INVALID, "problem or plan pointer is NULL");
-  *out = nullptr;
+// Checks of a problem shared by every entry point that takes one.
+int validate_problem(const lrd_problem* pr) {
   const int dims[3] = {pr->nx, pr->ny, pr->nz};
   const int pat[3] = {pr->px, pr->py, pr->pz};
   for (int a = 0; a < 3; ++a) {
@@ -504,6 +499,8 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   if (pr->form != LRD_FORM_PLAIN && pr->form != LRD_FORM_ACCURATE && pr->form != LRD_FORM_TENSOR)
     return fail(LRD_ERR_INVALID, "unknown form %d", pr->form);
   if (pr->batch < 0) return fail(LRD_ERR_INVALID, "batch must be >= 0, got %d", pr->batch);
+  if (pr->recon_split != 0 && pr->recon_split != 1 && pr->recon_split != 2 && pr->recon_split != 4)
+    return fail(LRD_ERR_INVALID, "recon_split must be 0, 1, 2 or 4, got %d", pr->recon_split);
   const long long nvox = (long long)pr->nx * pr->ny * pr->nz;
   if (nvox * pr->nt >= (1LL << 40)) return fail(LRD_ERR_UNSUPPORTED, "volume too large");
   const long long nvp = (long long)pr->px * pr->py * pr->pz;
@@ -511,6 +508,50 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   if (nvp < pr->nt)
     return fail(LRD_ERR_UNSUPPORTED,
                 "patch has %lld voxels < %d frames: the Gram route needs N >= T", nvp, pr->nt);
+  return LRD_OK;
+}
+
+// Reconstruction layout of a problem: threads per voxel, frames per thread
+// and the brick - the cost model's choice, or the problem's recon_split and
+// brick when set (a brick must fit the reconstruction kernel's threads per
+// CTA).
+int pick_layout(const lrd_problem* pr, const int dims[3], const int pat[3], const std::vector<int32_t> corners[3],
+                int& rsplit, int& rtpt, int best[3]) {
+  pick_recon_layout(pr->nt, pr->recon_split, pr->form != LRD_FORM_PLAIN, rsplit, rtpt);
+  choose_brick(dims, pat, corners, rsplit, best);
+  if (pr->brick_x > 0 || pr->brick_y > 0 || pr->brick_z > 0) {
+    if (pr->brick_x < 1 || pr->brick_y < 1 || pr->brick_z < 1 ||
+        (long long)pr->brick_x * pr->brick_y * pr->brick_z * rsplit > 1024)
+      return fail(LRD_ERR_INVALID, "brick %dx%dx%d: each side >= 1 and at most 256 voxels", pr->brick_x,
+                  pr->brick_y, pr->brick_z);
+    best[0] = pr->brick_x;
+    best[1] = pr->brick_y;
+    best[2] = pr->brick_z;
+    // the CTA must also fit the reconstruction kernel's registers
+    cudaFuncAttributes fa{};
+    for (bool acc : {false, true}) {
+      cudaError_t fe = cudaFuncGetAttributes(&fa, recon_kernel_ptr(rtpt, rsplit, acc));
+      if (fe != cudaSuccess) return cuda_fail(fe, "cudaFuncGetAttributes(recon_kernel)");
+      if ((long long)pr->brick_x * pr->brick_y * pr->brick_z * rsplit > fa.maxThreadsPerBlock)
+        return fail(LRD_ERR_INVALID, "brick %dx%dx%d x %d threads per voxel exceeds the reconstruction kernel's %d "
+                    "threads per CTA", pr->brick_x, pr->brick_y, pr->brick_z, rsplit, fa.maxThreadsPerBlock);
+    }
+  }
+  return LRD_OK;
+}
+
+// Plan for ``pr``; ``x_corners`` (nullable) replaces the x-axis corner list
+// (a slab of a larger volume), which must be sorted, start >= 0 and end
+// with a patch inside the volume.
+int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lrd_plan** out) {
+  g_last_error.clear();
+  if (!pr || !out) return fail(LRD_ERR_INVALID, "problem or plan pointer is NULL");
+  *out = nullptr;
+  if (int vrc = validate_problem(pr)) return vrc;
+  const int dims[3] = {pr->nx, pr->ny, pr->nz};
+  const int pat[3] = {pr->px, pr->py, pr->pz};
+  const long long nvox = (long long)pr->nx * pr->ny * pr->nz;
+  const long long nvp = (long long)pr->px * pr->py * pr->pz;
 
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -536,28 +577,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   // brick shape
   int best[3] = {1, 1, 1};
   int rsplit = 1, rtpt = 4;
-  if (pr->recon_split != 0 && pr->recon_split != 1 && pr->recon_split != 2 && pr->recon_split != 4)
-    return fail(LRD_ERR_INVALID, "recon_split must be 0, 1, 2 or 4, got %d", pr->recon_split);
-  pick_recon_layout(pr->nt, pr->recon_split, pr->form != LRD_FORM_PLAIN, rsplit, rtpt);
-  choose_brick(dims, pat, corners, rsplit, best);
-  if (pr->brick_x > 0 || pr->brick_y > 0 || pr->brick_z > 0) {
-    if (pr->brick_x < 1 || pr->brick_y < 1 || pr->brick_z < 1 ||
-        (long long)pr->brick_x * pr->brick_y * pr->brick_z * rsplit > 1024)
-      return fail(LRD_ERR_INVALID, "brick %dx%dx%d: each side >= 1 and at most 256 voxels", pr->brick_x,
-                  pr->brick_y, pr->brick_z);
-    best[0] = pr->brick_x;
-    best[1] = pr->brick_y;
-    best[2] = pr->brick_z;
-    // the CTA must also fit the reconstruction kernel's registers
-    cudaFuncAttributes fa{};
-    for (bool acc : {false, true}) {
-      cudaError_t fe = cudaFuncGetAttributes(&fa, recon_kernel_ptr(rtpt, rsplit, acc));
-      if (fe != cudaSuccess) return cuda_fail(fe, "cudaFuncGetAttributes(recon_kernel)");
-      if ((long long)pr->brick_x * pr->brick_y * pr->brick_z * rsplit > fa.maxThreadsPerBlock)
-        return fail(LRD_ERR_INVALID, "brick %dx%dx%d x %d threads per voxel exceeds the reconstruction kernel's %d "
-                    "threads per CTA", pr->brick_x, pr->brick_y, pr->brick_z, rsplit, fa.maxThreadsPerBlock);
-    }
-  }
+  if (int lrc = pick_layout(pr, dims, pat, corners, rsplit, rtpt, best)) return lrc;
   const int bsz[3] = {best[0], best[1], best[2]};
   for (int a = 0; a < 3; ++a) {
     const int nb = (dims[a] + bsz[a] - 1) / bsz[a];

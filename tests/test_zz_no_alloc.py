@@ -24,6 +24,11 @@ from lowrank_gpu_fastest_b200 import _native, api, problem, rel_l2
 pytestmark = pytest.mark.gpu
 
 PLAIN_TOL = 2e-7
+# relative L2 between the static path and lrd_denoise, per form: both follow the
+# same arithmetic except the Gram (per-patch kernel here, column kernel in the
+# plan path; for the tensor form the plan path's Gram is tcgen05 3xTF32)
+FORM_TOL = {0: PLAIN_TOL, 1: 1e-7, 2: 1e-7}
+FORM_NAME = {0: "plain", 1: "accurate", 2: "tensor"}
 
 
 def _problem(shape, patch, stride, form=0):
@@ -43,23 +48,35 @@ def _static_call(vol_dev, patch, stride, form=0):
     return out.cpu().numpy(), ranks.cpu().numpy()
 
 
-def test_static_entry_matches_plan_entry_twice(cuda_ok):
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_static_entry_matches_plan_entry_twice(cuda_ok, form):
     g = load_golden("config1_lowrank")
     vol = torch.from_numpy(golden_input(g)).cuda()
-    ref, ref_ranks = api.denoise(vol, (11, 11, 11), 3, return_ranks=True)
+    name = FORM_NAME[form]
+    ref, ref_ranks = api.denoise(vol, (11, 11, 11), 3, form=name, return_ranks=True)
     torch.cuda.synchronize()
     ref, ref_ranks = ref.cpu().numpy(), ref_ranks.cpu().numpy()
     other = torch.from_numpy(golden_input(load_golden("lowrank_p5s2"))).cuda()
     for call in range(2):
-        out, ranks = _static_call(vol, (11, 11, 11), 3)
+        out, ranks = _static_call(vol, (11, 11, 11), 3, form)
         np.testing.assert_array_equal(ranks, ref_ranks)
         assert np.isfinite(out).all()
-        assert rel_l2(out, ref) <= PLAIN_TOL, f"call {call}"
+        assert rel_l2(out, ref) <= FORM_TOL[form], f"call {call}"
         # a different problem through the same static array in between
-        o2, r2 = _static_call(other, (5, 5, 5), 2)
-        ref2, rr2 = api.denoise(other, (5, 5, 5), 2, return_ranks=True)
+        o2, r2 = _static_call(other, (5, 5, 5), 2, form)
+        ref2, rr2 = api.denoise(other, (5, 5, 5), 2, form=name, return_ranks=True)
         np.testing.assert_array_equal(r2, rr2.cpu().numpy())
-        assert rel_l2(o2, ref2.cpu().numpy()) <= PLAIN_TOL
+        assert rel_l2(o2, ref2.cpu().numpy()) <= FORM_TOL[form]
+
+
+def test_static_entry_rejects_overlapping_buffers(cuda_ok):
+    lib = _native.load()
+    vol = torch.zeros(16, 16, 16, 16, device="cuda")
+    pr = _problem((16, 16, 16, 16), (5, 5, 5), 2)
+    rc = lib.lrd_denoise_static(ctypes.byref(pr), vol.data_ptr(), vol.data_ptr(), None,
+                                torch.cuda.current_stream().cuda_stream)
+    assert rc == _native.LRD_ERR_INVALID
+    assert b"overlap" in lib.lrd_last_error_string()
 
 
 def test_static_entry_rejects_problems_beyond_its_scratch(cuda_ok):
