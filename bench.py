@@ -961,8 +961,10 @@ def run_sharded(args, wl):
 
 
 def run_batched(args):
-    """Batched uneven form: ``--volumes`` seeded volumes of mixed shapes in one
-    CUDA-graph launch per step (device-timed)."""
+    """Batched uneven form: ``--volumes`` seeded volumes of mixed shapes, the
+    whole batch one CUDA-graph launch of packed kernels per step
+    (device-timed), against the same volumes denoised one by one (the sum of
+    their single-volume device times)."""
     import torch
 
     from lowrank_gpu_fastest_b200 import api
@@ -976,26 +978,42 @@ def run_batched(args):
     patches = [r["patch"] for r in shapes]
     strides = [r["stride"] for r in shapes]
     P = sum(n_patches(r["shape"], r["patch"], r["stride"]) for r in shapes)
+
+    def timed(fn, reps):
+        out = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            out.append(s.elapsed_time(e))
+        return out
+
     for _ in range(args.warmup):
         api.denoise_batch(vols, patches, strides, use_graph=True)
     torch.cuda.synchronize()
-    times = []
-    for _ in range(args.steps):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        api.denoise_batch(vols, patches, strides, use_graph=True)
-        e.record()
-        torch.cuda.synchronize()
-        times.append(s.elapsed_time(e))
+    times = timed(lambda: api.denoise_batch(vols, patches, strides, use_graph=True), args.steps)
     ms = statistics.mean(times)
+    bp = next(iter(api._batch_plans.values()))
+    # the same volumes one by one (device-resident lrd_denoise each, warm plans)
+    single = []
+    for v, pt, st in zip(vols, patches, strides):
+        api.denoise(v, pt, st)
+        torch.cuda.synchronize()
+        single.append(min(timed(lambda: api.denoise(v, pt, st), 2)))
     N = [int(np.prod(r["patch"])) for r in shapes]
     flops = sum(4 * n * r["shape"][3] ** 2 * n_patches(r["shape"], r["patch"], r["stride"]) for n, r in zip(N, shapes))
     print(json.dumps(dict(
         metric="patches_per_s", workload="batched", value=P / (ms * 1e-3), unit="patches/s", n_gpus=1,
         steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, dtype="f32", data="synthetic",
+        single_volume_ms_sum=sum(single), vs_single_volumes=sum(single) / ms,
+        gpu_launches=bp.launches * args.steps, launches_per_batch=bp.launches,
+        launches_one_by_one=6 * len(shapes),
         config=dict(volumes=args.volumes, seed=args.seed, patches=P, algorithmic_tflop=flops / 1e12,
                     shapes=[[list(r["shape"]), r["patch"][0], r["stride"]] for r in shapes],
-                    note="one lrd_batch_denoise CUDA-graph launch per step, volumes on 4 internal streams"),
+                    note="one lrd_batch_denoise CUDA-graph launch per step: packed kernels, one grid per phase and "
+                         "kernel class across the volumes"),
         achieved_tflops=flops / (ms * 1e-3) / 1e12)), flush=True)
 
 

@@ -204,19 +204,34 @@ int lrd_denoise_static(const lrd_problem* problem, const float* d_vol, float* d_
  * over volumes (step8_tuned.py:116-146 per volume).
  *
  * lrd_batch_plan_create builds one plan per problem (the problems' brick and
- * split fields may carry autotuned values) and ``n_streams`` internal streams.
- * lrd_batch_denoise forks from ``stream`` onto the internal streams (volume i
- * on stream i mod n_streams, so small volumes overlap on the device), runs
- * every volume's pipeline, joins back into ``stream``. d_vols, d_outs and
- * d_ranks are host arrays of n device pointers (d_ranks and its entries may be
- * NULL); the workspace is one allocation of lrd_batch_workspace_size bytes.
- * With ``use_graph`` the whole batch is captured once into a CUDA graph and
- * later calls with the same pointers replay it as a single graph launch
- * (different pointers re-capture). No host synchronisation. */
+ * split fields may carry autotuned values) and groups the volumes' kernels
+ * into packed launches: per phase, one grid covers every volume of a kernel
+ * class (centring: all volumes; column Gram: per frame count; eigensolver:
+ * per solver class T <= 32 / 48 / 64 / 96 / 128; near-tie pass: all;
+ * reconstruction: per frame count and form), each block finding its volume
+ * in a device table of per-volume descriptors. Volumes whose Gram or
+ * reconstruction runs on another kernel (T % 4 != 0, the tcgen05 Gram of the
+ * tensor form, an explicit brick) get per-volume launches in that phase.
+ * Every volume's result is bit-identical to lrd_denoise's. ``n_streams`` is
+ * accepted for compatibility and unused: the launches run in order on
+ * ``stream``.
+ *
+ * lrd_batch_denoise runs the batch; d_vols, d_outs and d_ranks are host
+ * arrays of n device pointers (d_ranks and its entries may be NULL); the
+ * workspace is one allocation of lrd_batch_workspace_size bytes. Without
+ * ``use_graph`` the call copies the descriptor table from pinned staging
+ * memory (stream-ordered) and launches; with ``use_graph`` the launches are
+ * captured once into a CUDA graph with its own device table and later calls
+ * with the same pointers replay it as a single graph launch (different
+ * pointers re-capture). No host synchronisation on the replay path. One call
+ * at a time per batch plan. lrd_batch_num_launches gives the kernel launches
+ * of one call (17 for the 24 mixed-shape volumes of the batched benchmark,
+ * against 6 per volume one by one). */
 typedef struct lrd_batch_plan lrd_batch_plan;
 int lrd_batch_plan_create(const lrd_problem* problems, int32_t n, int32_t n_streams, lrd_batch_plan** plan);
 int lrd_batch_plan_destroy(lrd_batch_plan* plan);
 int lrd_batch_workspace_size(const lrd_batch_plan* plan, size_t* bytes);
+int lrd_batch_num_launches(const lrd_batch_plan* plan, int32_t* launches);
 int lrd_batch_denoise(lrd_batch_plan* plan, const float* const* d_vols, float* const* d_outs,
                       int32_t* const* d_ranks, void* d_workspace, void* stream, int32_t use_graph);
 

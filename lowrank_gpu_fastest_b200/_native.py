@@ -45,6 +45,7 @@ SIGNATURES = {
                                              ctypes.POINTER(ctypes.c_void_p)]),
     "lrd_batch_plan_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "lrd_batch_workspace_size": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t)]),
+    "lrd_batch_num_launches": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
     "lrd_batch_denoise": (ctypes.c_int, [ctypes.c_void_p] * 6 + [ctypes.c_int32]),
     "lrd_workspace_status": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
                                             ctypes.c_void_p]),
@@ -223,7 +224,8 @@ class SlabPlan(Plan):
 
 
 class BatchPlan:
-    """Owns an ``lrd_batch_plan*``: many problems, internal streams, a CUDA graph."""
+    """Owns an ``lrd_batch_plan*``: many problems in packed launches (one grid
+    per phase and kernel class), optionally one CUDA graph."""
 
     def __init__(self, problems, n_streams=4):
         """``problems``: list of dicts with shape, patch, stride, form, batch,
@@ -245,6 +247,9 @@ class BatchPlan:
         ws = ctypes.c_size_t()
         check(lib.lrd_batch_workspace_size(h, ctypes.byref(ws)))
         self.workspace_bytes = int(ws.value)
+        nl = ctypes.c_int32()
+        check(lib.lrd_batch_num_launches(h, ctypes.byref(nl)))
+        self.launches = int(nl.value)
 
     def __del__(self):
         h = getattr(self, "handle", None)

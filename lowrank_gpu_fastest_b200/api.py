@@ -160,9 +160,11 @@ def denoise_batch(vols, patches=(11, 11, 11), strides=3, *, form="plain", use_gr
 
     ``vols``: list of float32 CUDA tensors (device-resident; outputs are CUDA
     tensors) or numpy arrays (copied in and out). ``patches`` / ``strides``:
-    one value for all volumes or one per volume. Volume i runs on internal
-    stream i mod ``n_streams``; with ``use_graph`` the whole batch is one
-    CUDA-graph launch, captured on the first call with these buffers. With
+    one value for all volumes or one per volume. The volumes run in packed
+    launches - one grid per phase and kernel class across all of them
+    (``lrd_batch_*``; ``n_streams`` is kept for compatibility and unused);
+    with ``use_graph`` the whole batch is one CUDA-graph launch, captured on
+    the first call with these buffers. With
     ``autotune`` each distinct (frames, patch, stride) gets its reconstruction
     launch shape from :func:`lowrank_gpu_fastest_b200.tune.tune`.
     """

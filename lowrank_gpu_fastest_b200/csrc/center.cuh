@@ -47,15 +47,17 @@ __device__ __forceinline__ float np_pairwise_sum_row(const float* row, int n) {
 // coalesced; each lane then reduces one row.
 // grid: ceil(nvox / (32 * warps_per_block)) blocks of 32*warps_per_block threads,
 // dynamic smem: warps_per_block * (32 * (T + 1) + 32) floats.
-__global__ void center_kernel(const float* __restrict__ vol, float* __restrict__ xc,
-                              float* __restrict__ mean, long long nvox, int T) {
+// Body of one block (index ``bid``); shared by the single-volume kernel below
+// and the packed multi-volume launch (batch.cuh).
+__device__ __forceinline__ void center_body(const float* __restrict__ vol, float* __restrict__ xc,
+                                            float* __restrict__ mean, long long nvox, int T, long long bid) {
   extern __shared__ float smem_center[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int ld = T + 1;  // odd stride: lane-per-row reads are conflict-free
   float* s = smem_center + (size_t)warp * (32 * ld + 32);
   float* s_mean = s + 32 * ld;
-  const long long v0 = ((long long)blockIdx.x * (blockDim.x >> 5) + warp) * 32;
+  const long long v0 = (bid * (blockDim.x >> 5) + warp) * 32;
   if (v0 >= nvox) return;  // whole warp leaves; no block-level barrier below
   const int nrows = (int)min(32LL, nvox - v0);
   const int nval = nrows * T;
@@ -88,6 +90,11 @@ __global__ void center_kernel(const float* __restrict__ vol, float* __restrict__
       if (t >= T) { t -= T; ++r; }
     }
   }
+}
+
+__global__ void center_kernel(const float* __restrict__ vol, float* __restrict__ xc,
+                              float* __restrict__ mean, long long nvox, int T) {
+  center_body(vol, xc, mean, nvox, T, blockIdx.x);
 }
 
 }  // namespace lrd

@@ -531,10 +531,12 @@ constexpr int kRefinePrefetch = 16; // floats of the next z-run a thread prefetc
 // patch's rank, weight, eigenvectors (and eigenvalues if requested). A queue
 // holds a handful of patches per volume, so this pass is one patch's latency:
 // every step of it is spread over the block.
-__global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, float* __restrict__ lam_out,
-                                   int32_t* __restrict__ ranks, float* __restrict__ wgt, float* __restrict__ sig2,
-                                   Geom g, AxisTables tab, const int* __restrict__ refine_count,
-                                   const int* __restrict__ refine_ids) {
+// Body: this block is block ``bid`` of ``nblocks`` working on one volume's queue.
+__device__ __forceinline__ void eigh_refine_body(const float* __restrict__ xc, float* vecs,
+                                                 float* __restrict__ lam_out, int32_t* __restrict__ ranks,
+                                                 float* __restrict__ wgt, float* __restrict__ sig2, const Geom& g,
+                                                 const AxisTables& tab, const int* __restrict__ refine_count,
+                                                 const int* __restrict__ refine_ids, int bid, int nblocks) {
   extern __shared__ double sm_ref[];
   const int n = g.nt;
   const int lda = eigh_lda(n);
@@ -551,7 +553,7 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
   // the next run goes through registers while this one is used (one barrier
   // per run) when a thread's share fits kRefinePrefetch floats
   const bool prefetch = runlen <= kRefinePrefetch * nth;
-  for (int w = first + blockIdx.x; w < count; w += gridDim.x) {
+  for (int w = first + bid; w < count; w += nblocks) {
     const long long pid = refine_ids[w];
     int ci, cj, ck;
     patch_axes(g, pid, ci, cj, ck);
@@ -631,6 +633,14 @@ __global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, fl
                           sig2 ? sig2 + pid : nullptr);
     __syncthreads();
   }
+}
+
+__global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, float* __restrict__ lam_out,
+                                   int32_t* __restrict__ ranks, float* __restrict__ wgt, float* __restrict__ sig2,
+                                   Geom g, AxisTables tab, const int* __restrict__ refine_count,
+                                   const int* __restrict__ refine_ids) {
+  eigh_refine_body(xc, vecs, lam_out, ranks, wgt, sig2, g, tab, refine_count, refine_ids, (int)blockIdx.x,
+                   (int)gridDim.x);
 }
 
 // Marks every queued near-tie patch as refined (one thread).

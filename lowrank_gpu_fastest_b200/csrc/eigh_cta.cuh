@@ -90,14 +90,15 @@ __device__ __forceinline__ int sturm_count1(const float* __restrict__ d, const f
   return a;
 }
 
-// grid: one CTA of TMAX threads per patch of this launch (patch index
-// patch0 + blockIdx.x), n <= TMAX. ``gram`` (read) and ``vecs`` (written) may
+// One CTA of TMAX threads per patch: the body solves the launch's patch ``b``
+// (patch index patch0 + b), n <= TMAX. ``gram`` (read) and ``vecs`` (written) may
 // alias: the CTA reads its whole matrix before writing.
 template <int TMAX>
-__global__ void __launch_bounds__(TMAX)
-    eigh_cta_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
-                    float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
-                    int* __restrict__ refine_count, int* __restrict__ refine_ids) {
+__device__ __forceinline__ void eigh_cta_body(const float* gram, float* vecs, float* __restrict__ lam_out,
+                                              int32_t* __restrict__ ranks, float* __restrict__ wgt,
+                                              float* __restrict__ sig2, int n, int nvox, long long patch0,
+                                              int* __restrict__ refine_count, int* __restrict__ refine_ids,
+                                              long long b) {
   constexpr int NW = TMAX / 32;
   extern __shared__ __align__(16) float sc[];
   float* HV = sc;  // packed reflector vectors
@@ -112,7 +113,6 @@ __global__ void __launch_bounds__(TMAX)
   float* xk = W;                          // tridiagonalisation only: row k broadcast
   float* ws = W + TMAX;                   //   and the w vector
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long long b = blockIdx.x;
   const float* G = gram + b * (long long)n * n;
   const bool rv = tid < n;
   LRD_STAMP(0);
@@ -438,6 +438,15 @@ __global__ void __launch_bounds__(TMAX)
     __syncthreads();  // the next chunk's Gram-Schmidt reads these rows
   }
   LRD_STAMP(7);
+}
+
+template <int TMAX>
+__global__ void __launch_bounds__(TMAX)
+    eigh_cta_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
+                    float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
+                    int* __restrict__ refine_count, int* __restrict__ refine_ids) {
+  eigh_cta_body<TMAX>(gram, vecs, lam_out, ranks, wgt, sig2, n, nvox, patch0, refine_count, refine_ids,
+                      (long long)blockIdx.x);
 }
 
 }  // namespace lrd

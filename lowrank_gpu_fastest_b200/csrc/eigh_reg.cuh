@@ -184,11 +184,14 @@ __device__ __forceinline__ void bisect_reg(const float* d, const float* e, const
   tnorm_out = tnorm;
 }
 
+// Body of one warp's matrix ``b`` (the launch's patch index; the patch is
+// patch0 + b), shared by the single-volume kernel and the packed launch.
 template <int TMAX>
-__global__ void __launch_bounds__(32)
-    eigh_reg_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
-                    float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
-                    int* __restrict__ refine_count, int* __restrict__ refine_ids) {
+__device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, float* __restrict__ lam_out,
+                                              int32_t* __restrict__ ranks, float* __restrict__ wgt,
+                                              float* __restrict__ sig2, int n, int nvox, long long patch0,
+                                              int* __restrict__ refine_count, int* __restrict__ refine_ids,
+                                              long long b) {
   constexpr int NR = eigh_reg_nr<TMAX>();
   extern __shared__ __align__(16) float sr[];
   float* HV = sr;  // packed reflector vectors
@@ -202,7 +205,6 @@ __global__ void __launch_bounds__(32)
   float* xk = W;                         // tridiagonalisation only: row k broadcast
   float* ws = W + TMAX;                  //   and the w vector
   const int lane = threadIdx.x;
-  const long long b = blockIdx.x;
   const float* G = gram + b * (long long)n * n;
   LRD_STAMP(0);
 
@@ -540,6 +542,15 @@ __global__ void __launch_bounds__(32)
     __syncwarp();
   }
   LRD_STAMP(7);
+}
+
+template <int TMAX>
+__global__ void __launch_bounds__(32)
+    eigh_reg_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
+                    float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
+                    int* __restrict__ refine_count, int* __restrict__ refine_ids) {
+  eigh_reg_body<TMAX>(gram, vecs, lam_out, ranks, wgt, sig2, n, nvox, patch0, refine_count, refine_ids,
+                      (long long)blockIdx.x);
 }
 
 }  // namespace lrd

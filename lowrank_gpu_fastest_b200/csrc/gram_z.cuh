@@ -108,8 +108,8 @@ __host__ __device__ inline int gramz_threads(int T, int ks) {
   return ((nb * (nb + 1) / 2 * ks) + 31) & ~31;
 }
 
-// grid: nfull + (columns - nfull) * nsplit CTAs; block: gramz_threads(T, ks)
-// (T % 4 == 0, ks in {1, 2, 4}). CTA b < nfull computes every window of column
+// grid: nfull + (columns - nfull) * nsplit CTAs; block: gramz_threads(T, KS)
+// (T % 4 == 0, KS in {1, 2, 4}). CTA b < nfull computes every window of column
 // col0 + b; the columns after the first nfull are each cut into nsplit units
 // of consecutive windows (a unit reads only the planes of its windows), so a
 // launch whose last wave would hold a few whole columns spreads that tail
@@ -117,9 +117,14 @@ __host__ __device__ inline int gramz_threads(int T, int ks) {
 // result does not depend on the cut. ``col0`` = first column (x-major index
 // ci * ncy + cj); ``gram`` points at the Gram block of the launch's first
 // patch (patch index col0 * ncz).
-__global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g,
-                              AxisTables tab, long long col0, int ring, int ks, int nfull, int nsplit,
-                              int* status) {
+// Body of one CTA (index ``bid``); ``xmap`` points at the tensor map (a kernel
+// parameter, or a 64-byte aligned copy in global memory for the packed
+// multi-volume launch).
+template <int KS>
+__device__ __forceinline__ void gram_z_body(const CUtensorMap* xmap, float* __restrict__ gram, const Geom& g,
+                                            const AxisTables& tab, long long col0, int ring, int nfull, int nsplit,
+                                            int* status, int bid) {
+  constexpr int ks = KS;
   extern __shared__ __align__(128) float smz[];
   const int T = g.nt;
   const int rows = g.px * g.py;
@@ -135,7 +140,6 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
   const uint32_t bar1 = (uint32_t)__cvta_generic_to_shared(&bars[1]);
 
   // this CTA's column and windows [wlo, whi]
-  const int bid = (int)blockIdx.x;
   const bool cut = bid >= nfull;
   const int u = cut ? bid - nfull : 0, nparts = cut ? nsplit : 1, part = u % nparts;
   const long long col = col0 + (cut ? nfull + u / nparts : bid);
@@ -155,8 +159,7 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
     }
     bj = bi + rem;
   }
-  const int ucount = 16 / ks;      // window entries this thread updates
-  const int ubase = kq * ucount;
+  constexpr int ucount = 16 / ks;  // window entries this thread updates: [kq * ucount, kq * ucount + ucount)
   const uint32_t plane_bytes = (uint32_t)(rows * T * sizeof(float));
 
   for (int e = tid; e < ring * 16 * nblk; e += nthreads) win[e] = 0.f;
@@ -168,7 +171,7 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
   __syncthreads();
   if (tid == 0 && zlo <= zhi) {
     mbar_expect_tx(bar0, plane_bytes);
-    tma_load_4d((uint32_t)__cvta_generic_to_shared(plane0), &xmap, bar0, 0, zlo, cy, cx);
+    tma_load_4d((uint32_t)__cvta_generic_to_shared(plane0), xmap, bar0, 0, zlo, cy, cx);
   }
   float* G0 = gram + (size_t)((col - col0) * g.ncz) * T * T;
   int gave_up = 0;  // uniform: a wait of some thread gave up at plane stop_z
@@ -183,7 +186,7 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
       const uint32_t nb_ = slot ? bar0 : bar1;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       mbar_expect_tx(nb_, plane_bytes);
-      tma_load_4d((uint32_t)__cvta_generic_to_shared(slot ? plane0 : plane1), &xmap, nb_, 0, z + 1, cy, cx);
+      tma_load_4d((uint32_t)__cvta_generic_to_shared(slot ? plane0 : plane1), xmap, nb_, 0, z + 1, cy, cx);
     }
     const bool ok = mbar_wait_bounded(slot ? bar1 : bar0, (uint32_t)((it >> 1) & 1), status);
     const int klo = max(tab.cover[2][2 * z], wlo), khi = min(tab.cover[2][2 * z + 1], whi);
@@ -215,29 +218,38 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
         for (int u = 0; u < 16; ++u) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], 2);
       }
       if (owner) {
-        for (int k = klo; k <= khi; ++k) {
-          float* w = win + (size_t)(k % ring) * 16 * nblk + blk;
-          const bool last = z == tab.corners[2][k] + g.pz - 1;
-          if (!last) {
+        // this thread's entries of the 4x4 block, e = kq * ucount + q
+        float mine[ucount];
 #pragma unroll
-            for (int u = 0; u < 16; ++u)
-              if (u >= ubase && u < ubase + ucount) w[u * nblk] += acc[u];
+        for (int q = 0; q < ucount; ++q) {
+          float v = acc[q];
+#pragma unroll
+          for (int c = 1; c < ks; ++c)
+            if (kq == c) v = acc[c * ucount + q];
+          mine[q] = v;
+        }
+        // Windows are consecutive and their corners increase, so only the
+        // lowest window holding plane z (klo) can end at z.
+        const bool klo_ends = z == tab.corners[2][klo] + g.pz - 1;
+        int slot = klo % ring;
+        for (int k = klo; k <= khi; ++k) {
+          float* w = win + (size_t)slot * 16 * nblk + blk + (size_t)kq * ucount * nblk;
+          if (k != klo || !klo_ends) {
+#pragma unroll
+            for (int q = 0; q < ucount; ++q) w[q * nblk] += mine[q];
           } else {
             float* G = G0 + (size_t)k * T * T;
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-              for (int v = 0; v < 4; ++v) {
-                const int e = u * 4 + v;
-                if (e >= ubase && e < ubase + ucount) {
-                  const float val = w[e * nblk] + acc[e];
-                  w[e * nblk] = 0.f;
-                  const int r = bi * 4 + u, c = bj * 4 + v;
-                  G[(size_t)r * T + c] = val;
-                  G[(size_t)c * T + r] = val;
-                }
-              }
+            for (int q = 0; q < ucount; ++q) {
+              const int e = kq * ucount + q;
+              const float val = w[q * nblk] + mine[q];
+              w[q * nblk] = 0.f;
+              const int r = bi * 4 + (e >> 2), c = bj * 4 + (e & 3);
+              G[(size_t)r * T + c] = val;
+              G[(size_t)c * T + r] = val;
+            }
           }
+          if (++slot == ring) slot = 0;
         }
       }
     }
@@ -254,6 +266,13 @@ __global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMa
     drain_copies(!own_wait_ok, slot ? bar1 : bar0, (uint32_t)((it >> 1) & 1), stop_z + 1 <= zhi,
                  slot ? bar0 : bar1, (uint32_t)(((it + 1) >> 1) & 1), status);
   }
+}
+
+template <int KS>
+__global__ void __maxnreg__(64) gram_z_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g,
+                              AxisTables tab, long long col0, int ring, int nfull, int nsplit,
+                              int* status) {
+  gram_z_body<KS>(&xmap, gram, g, tab, col0, ring, nfull, nsplit, status, (int)blockIdx.x);
 }
 
 // Self-test of the bounded wait: one thread waits on a freshly initialised

@@ -24,6 +24,7 @@
 #include "gram_z.cuh"
 #include "lrd_common.cuh"
 #include "recon.cuh"
+#include "recon_warp.cuh"
 
 namespace {
 
@@ -69,6 +70,7 @@ struct lrd_plan {
   long long nvox;
   int tpt;                 // recon frames per thread
   int split;               // recon threads per voxel
+  bool recon_warp = false; // reconstruction by recon_warp_kernel (2 x 2 x 2 voxels per warp)
   int gram_threads;
   bool use_gramz;          // column Gram kernel (TMA-staged z-planes) instead of per-patch
   bool use_gramtc;         // the column Gram on tcgen05 (tensor form)
@@ -121,6 +123,14 @@ namespace {
 // against 0.96 ms unsplit and 1.27 ms with 4; T = 32, 64 and 96 are fastest
 // unsplit (0.58 / 1.44 / 1.21 ms, the split costing 30-60%).
 int gramz_split(int T) { return (T > 40 && T <= 56) ? 2 : 1; }
+
+void* gramz_kernel_ptr(int ks) {
+  switch (ks) {
+    case 2: return (void*)lrd::gram_z_kernel<2>;
+    case 4: return (void*)lrd::gram_z_kernel<4>;
+    default: return (void*)lrd::gram_z_kernel<1>;
+  }
+}
 
 // Reconstruction thread layout for T frames: two threads per voxel up to
 // T = 48, four above (a thread's frame slices, accumulators and projections
@@ -260,6 +270,16 @@ void* recon_kernel_ptr(int tpt, int split, bool accurate) {
   return nullptr;
 }
 
+void* recon_warp_ptr(int T, bool accurate) {
+  switch (T) {
+    case 32: return accurate ? (void*)lrd::recon_warp_kernel<8, true> : (void*)lrd::recon_warp_kernel<8, false>;
+    case 48: return accurate ? (void*)lrd::recon_warp_kernel<12, true> : (void*)lrd::recon_warp_kernel<12, false>;
+    case 64: return accurate ? (void*)lrd::recon_warp_kernel<16, true> : (void*)lrd::recon_warp_kernel<16, false>;
+    case 96: return accurate ? (void*)lrd::recon_warp_kernel<24, true> : (void*)lrd::recon_warp_kernel<24, false>;
+  }
+  return nullptr;
+}
+
 // The dynamic shared-memory limit is a property of the kernel, shared by
 // every plan in the process: only ever raise it (per device and kernel), so a
 // plan created later with a smaller need cannot shrink an earlier plan's.
@@ -374,9 +394,16 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
             map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, (int)nfull, nsplit, status);
         rc = launch_check("gram_tc_kernel launch");
       } else {
-        lrd::gram_z_kernel<<<(unsigned)grid, lrd::gramz_threads(P->g.nt, P->gramz_ks), P->smem_gramz, st>>>(
-            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, P->gramz_ks, (int)nfull, nsplit,
-            status);
+        void* fn = gramz_kernel_ptr(P->gramz_ks);
+        float* gout = d_gram + c0 * P->g.ncz * TT;
+        lrd::Geom gg = P->g;
+        lrd::AxisTables tt = P->tab;
+        int ring = P->gramz_ring, nf = (int)nfull;
+        void* args[] = {(void*)&map, (void*)&gout, (void*)&gg, (void*)&tt, (void*)&c0, (void*)&ring,
+                        (void*)&nf, (void*)&nsplit, (void*)&status};
+        cudaError_t le = cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(lrd::gramz_threads(P->g.nt, P->gramz_ks)),
+                                          args, P->smem_gramz, st);
+        if (le != cudaSuccess) return cuda_fail(le, "gram_z_kernel launch");
         rc = launch_check("gram_z_kernel launch");
       }
       if (rc) return rc;
@@ -460,8 +487,10 @@ int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long l
   const long long nbricks = (long long)P->g.nbx * P->g.nby * P->g.nbz;
   if (b_hi < 0) b_hi = nbricks;
   if (b_hi <= b_lo) return LRD_OK;
-  const unsigned threads = (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
-  void* fn = recon_kernel_ptr(P->tpt, P->split, acc);
+  const unsigned threads =
+      P->recon_warp ? 32u * lrd::kReconWarps : (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
+  void* fn = P->recon_warp ? recon_warp_ptr(P->g.nt, acc) : recon_kernel_ptr(P->tpt, P->split, acc);
+  const size_t smem = P->recon_warp ? 0 : P->smem_recon;
   lrd::Geom g = P->g;
   lrd::AxisTables tab = P->tab;
   int brick0 = (int)b_lo;
@@ -469,7 +498,7 @@ int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long l
   if (io) sio = *io;
   void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv, (void*)&rank, (void*)&wgt,
                   (void*)&d_out, (void*)&g, (void*)&tab, (void*)&brick0, (void*)&sio};
-  cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)(b_hi - b_lo)), dim3(threads), args, P->smem_recon, st);
+  cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)(b_hi - b_lo)), dim3(threads), args, smem, st);
   if (e != cudaSuccess) return cuda_fail(e, "recon_kernel launch");
   return LRD_OK;
 }
@@ -514,9 +543,23 @@ int validate_problem(const lrd_problem* pr) {
 // Reconstruction layout of a problem: threads per voxel, frames per thread
 // and the brick - the cost model's choice, or the problem's recon_split and
 // brick when set (a brick must fit the reconstruction kernel's threads per
-// CTA).
+// CTA). Without either, frame counts the warp kernel is built for take it
+// (``warp``; brick 2 x 2 x recon_warp_bz(), four lanes per voxel).
+// Measured on B200, reconstruction ms, 96x96x48x48 / 11^3 / stride 3:
+// brick kernel (3x3x3, 2 threads per voxel) 1.22 -> warp kernel (see DESIGN).
 int pick_layout(const lrd_problem* pr, const int dims[3], const int pat[3], const std::vector<int32_t> corners[3],
-                int& rsplit, int& rtpt, int best[3]) {
+                int& rsplit, int& rtpt, int best[3], bool* warp = nullptr) {
+  if (warp) *warp = false;
+  if (warp && pr->recon_split == 0 && pr->brick_x == 0 && pr->brick_y == 0 && pr->brick_z == 0 &&
+      lrd::recon_warp_supported(pr->nt)) {
+    *warp = true;
+    rsplit = 4;
+    rtpt = pr->nt / 4;
+    best[0] = 2;
+    best[1] = 2;
+    best[2] = lrd::recon_warp_bz();
+    return LRD_OK;
+  }
   pick_recon_layout(pr->nt, pr->recon_split, pr->form != LRD_FORM_PLAIN, rsplit, rtpt);
   choose_brick(dims, pat, corners, rsplit, best);
   if (pr->brick_x > 0 || pr->brick_y > 0 || pr->brick_z > 0) {
@@ -577,7 +620,8 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   // brick shape
   int best[3] = {1, 1, 1};
   int rsplit = 1, rtpt = 4;
-  if (int lrc = pick_layout(pr, dims, pat, corners, rsplit, rtpt, best)) return lrc;
+  bool warp_recon = false;
+  if (int lrc = pick_layout(pr, dims, pat, corners, rsplit, rtpt, best, &warp_recon)) return lrc;
   const int bsz[3] = {best[0], best[1], best[2]};
   for (int a = 0; a < 3; ++a) {
     const int nb = (dims[a] + bsz[a] - 1) / bsz[a];
@@ -642,6 +686,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   const int T = pr->nt;
   P->tpt = rtpt;
   P->split = rsplit;
+  P->recon_warp = warp_recon;
   const int nb4 = (T + 3) / 4;
   P->gram_threads = nb4 * (nb4 + 1) / 2;
   P->center_warps = 4;
@@ -663,7 +708,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   }
   int rc = set_smem((const void*)lrd::center_kernel, P->smem_center);
   if (!rc) rc = set_smem((const void*)lrd::gram_kernel, P->smem_gram);
-  if (!rc && P->use_gramz) rc = set_smem((const void*)lrd::gram_z_kernel, P->smem_gramz);
+  if (!rc && P->use_gramz) rc = set_smem(gramz_kernel_ptr(P->gramz_ks), P->smem_gramz);
   if (!rc && P->use_gramtc) rc = set_smem((const void*)lrd::gram_tc_kernel, P->smem_gramtc);
   P->smem_refine = lrd::eigh_refine_smem_bytes(T, pr->pz);
   if (!rc) rc = set_smem((const void*)lrd::eigh_refine_kernel, P->smem_refine);
@@ -674,7 +719,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     P->sms = sms;
     int per_sm = 0;
     if (!rc && P->use_gramz) {
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lrd::gram_z_kernel,
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gramz_kernel_ptr(P->gramz_ks),
                                                         lrd::gramz_threads(T, P->gramz_ks),
                                                         P->smem_gramz) == cudaSuccess)
         P->gramz_slots = per_sm * sms;

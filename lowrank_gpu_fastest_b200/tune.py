@@ -1,5 +1,9 @@
 """Autotuner for the reconstruction launch shape (brick and threads per voxel).
 
+Brick (0, 0, 0) with split 0 is the plan's own choice: the warp kernel (one
+warp per 2x2x2 voxel block) for the frame counts it is built for, else the
+brick kernel with the cost model's brick.
+
 The reconstruction kernel's speed depends on the brick of voxels a CTA owns
 (how many of the patches touching the brick actually cover each voxel, how
 many CTAs fit on an SM) and on how many threads share a voxel's frames. The
@@ -114,7 +118,9 @@ def tune(shape, patch=(11, 11, 11), stride=3, form="plain", device=None, max_can
 
     cands = candidates(T, patch, stride)
     cands.sort(key=lambda c: slots(c[0]) * c[1] / max(1, min(4, c[1])))
-    cands = cands[:max_candidates]
+    # the plan's own choice first (brick and split 0: the warp-per-2x2x2-block
+    # kernel where it is built for T, else the cost model's brick)
+    cands = [((0, 0, 0), 0)] + cands[:max_candidates]
     vol, _ = make_phantom_lowrank(tuple(int(v) for v in shape), seed=7)
     best, best_ms, results = None, float("inf"), []
     with torch.cuda.device(device):

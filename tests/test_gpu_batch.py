@@ -40,6 +40,15 @@ def test_batch_equals_single(cuda_ok, use_graph):
         assert torch.equal(r, sr)
 
 
+def test_packed_launch_count(cuda_ok):
+    """The batch runs in packed launches: far fewer than six per volume."""
+    from lowrank_gpu_fastest_b200 import _native
+
+    bp = _native.BatchPlan([dict(shape=s, patch=p, stride=st) for s, p, st in CASES])
+    print("launches per batch", bp.launches, "for", len(CASES), "volumes")
+    assert bp.launches < 6 * len(CASES)
+
+
 def test_batch_matches_oracle_ranks(cuda_ok):
     vols = _vols()
     outs, ranks = api.denoise_batch(vols, [c[1] for c in CASES], [c[2] for c in CASES], return_ranks=True)
