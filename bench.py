@@ -139,6 +139,8 @@ def phase_kernel(phase, T, form):
         return "gram_tc_kernel" if (form == "tensor" and T <= 64) else "gram_z_kernel"
     if phase == "eigh_mp":
         return "eigh_reg_kernel" if T <= 64 else "eigh_cta_kernel"
+    if phase == "recon" and T in (32, 48, 64, 96):
+        return "recon_warp_kernel"  # one warp per 2x2x2 voxel block (the plan's default layout)
     if phase == "recon" and form == "plain" and 45 <= T <= 48:
         return "recon_kernel_t24s2"  # 24 frames x 2 threads, built with 112 registers
     return {"center": "center_kernel", "recon": "recon_kernel"}[phase]
@@ -155,6 +157,10 @@ def parse():
     ap.add_argument("--volumes", type=int, default=24, help="batched: number of volumes")
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
     ap.add_argument("--rate", type=float, default=40.0, help="serving: Poisson arrival rate (req/s)")
+    ap.add_argument("--duration", type=float, default=0.0,
+                    help="serving: arrivals for this many seconds instead of --requests (config: 60)")
+    ap.add_argument("--serving-requests", type=int, default=12,
+                    help="headline line: requests of the bounded serving sample (0 = none)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-step8", action="store_true", help="skip the reference's step-8 GPU timing")
@@ -413,7 +419,6 @@ def time_form(torch, dist, args, wl, form, vol, rank, world, local, *, clocks=Fa
         sampler = ClockSampler(local)
         sampler.start()
         time.sleep(0.3)
-    plan.set_profiling(True)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
     if world > 1:
@@ -430,9 +435,16 @@ def time_form(torch, dist, args, wl, form, vol, rank, world, local, *, clocks=Fa
         dist.barrier()
     wall = time.perf_counter() - t_wall
     clk = sampler.stop() if sampler else None
+    status = plan.status(ws.data_ptr(), sid)
+    # phase times from separate profiled calls (a profiled call runs its phases one after
+    # another; the timed calls above overlap the phases of successive x-slabs)
+    plan.set_profiling(True)
+    for _ in range(min(args.steps, 5)):
+        flush.zero_()
+        step()
     phases, ncalls = plan.phase_ms()
     plan.set_profiling(False)
-    status = plan.status(ws.data_ptr(), sid)
+    torch.cuda.synchronize()
     t = torch.tensor([sum(s.elapsed_time(e) for s, e in evs)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -467,9 +479,11 @@ def time_form(torch, dist, args, wl, form, vol, rank, world, local, *, clocks=Fa
     e2e_ms_step = float(t.item())
     e2e_same = bool(np.array_equal(h_out.numpy(), out_np) and np.array_equal(h_ranks.numpy(), ranks_np))
     res = dict(form=form, P=P, ms_per_step=ms_per_step, value=world * P / (ms_per_step * 1e-3),
+               phases_sum_ms=None,
                e2e_ms=e2e_ms_step, e2e_value=world * P / (e2e_ms_step * 1e-3), wall=wall, clocks=clk,
                phases={k: v / max(ncalls, 1) for k, v in phases.items()}, status=status,
                e2e_output_identical=e2e_same, out=out_np, ranks=ranks_np, plan=plan)
+    res["phases_sum_ms"] = sum(res["phases"].values())
     if golden is not None:
         res["accuracy"] = golden_accuracy(out_np, ranks_np, golden)
     del d_vol, d_out, ws, flush, d_in, h_in, h_out
@@ -689,6 +703,14 @@ def run_ours(args, wl):
             vols["ladder_phantom"] = (vref, fixtures[1])
         libeigh = library_eigh(torch, wl, vol, local)
         step8 = reference_step8(torch, wl, vols, repeats=args.step8_repeats)
+    serving = None
+    if world == 1 and rank == 0 and args.serving_requests > 0 and not args.single_form:
+        try:
+            serving = serving_run(args.serving_requests, args.rate, args.seed)
+            serving["note"] = ("bounded sample of the serving stream; the full one is "
+                               "bench.py --workload serving --duration 60")
+        except Exception as exc:  # the headline numbers stand without it
+            serving = dict(error=f"{type(exc).__name__}: {exc}")
 
     if rank == 0:
         P = main["P"]
@@ -743,6 +765,8 @@ def run_ours(args, wl):
             line["ladder_phantom"] = {f: summary(r) for f, r in ladder.items()}
         if libeigh is not None:
             line["eigh_vs_library"] = libeigh
+        if serving is not None:
+            line["serving"] = serving
         if step8 is not None:
             line["reference_step8"] = step8
             lr = step8.get("lowrank")
@@ -995,20 +1019,31 @@ def run_batched(args):
     torch.cuda.synchronize()
     times = timed(lambda: api.denoise_batch(vols, patches, strides, use_graph=True), args.steps)
     ms = statistics.mean(times)
-    bp = next(iter(api._batch_plans.values()))
-    # the same volumes one by one (device-resident lrd_denoise each, warm plans)
+    launches = next(iter(api._batch_plans.values())).launches
+    api._batch_plans.clear()  # frees the batch's workspace (tens of GB for the stride-1 volumes)
+    torch.cuda.empty_cache()
+    # the same volumes one by one: lrd_denoise each on one shared workspace, warm plans
+    from lowrank_gpu_fastest_b200 import _native
+
+    plans = [_native.Plan(tuple(v.shape), pt, st) for v, pt, st in zip(vols, patches, strides)]
+    ws = torch.empty(max(p.workspace_bytes for p in plans), dtype=torch.uint8, device="cuda")
+    out = torch.empty(max(v.numel() for v in vols), dtype=torch.float32, device="cuda")
+    sid = torch.cuda.current_stream().cuda_stream
     single = []
-    for v, pt, st in zip(vols, patches, strides):
-        api.denoise(v, pt, st)
+    for v, plan in zip(vols, plans):
+        def one():
+            plan.denoise(v.data_ptr(), out.data_ptr(), None, ws.data_ptr(), sid)
+
+        one()
         torch.cuda.synchronize()
-        single.append(min(timed(lambda: api.denoise(v, pt, st), 2)))
+        single.append(min(timed(one, 2)))
     N = [int(np.prod(r["patch"])) for r in shapes]
     flops = sum(4 * n * r["shape"][3] ** 2 * n_patches(r["shape"], r["patch"], r["stride"]) for n, r in zip(N, shapes))
     print(json.dumps(dict(
         metric="patches_per_s", workload="batched", value=P / (ms * 1e-3), unit="patches/s", n_gpus=1,
         steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True, dtype="f32", data="synthetic",
         single_volume_ms_sum=sum(single), vs_single_volumes=sum(single) / ms,
-        gpu_launches=bp.launches * args.steps, launches_per_batch=bp.launches,
+        gpu_launches=launches * args.steps, launches_per_batch=launches,
         launches_one_by_one=6 * len(shapes),
         config=dict(volumes=args.volumes, seed=args.seed, patches=P, algorithmic_tflop=flops / 1e12,
                     shapes=[[list(r["shape"]), r["patch"][0], r["stride"]] for r in shapes],
@@ -1017,56 +1052,66 @@ def run_batched(args):
         achieved_tflops=flops / (ms * 1e-3) / 1e12)), flush=True)
 
 
-def run_serving(args):
-    """Serving form: ``--requests`` seeded requests arriving as a Poisson
-    stream at ``--rate`` req/s (10% 128x128x64x96 / 11^3 / stride 2), served
-    with continuous batching; compared with solving the same requests one
-    after another."""
+def serving_run(requests, rate, seed=0, duration=None, distinct=24, slots=4):
+    """Serving form: Poisson arrivals at ``rate`` req/s (``requests`` of them,
+    or as many as arrive within ``duration`` s) of the serving mix (x, y in
+    64..128, z in 32..64, T in {32, 48, 64, 96}, patch 5^3 / 7^3 / 11^3,
+    stride 1..3; 10% 128x128x64x96 / 11^3 / stride 2), submitted to a
+    ``Server`` as they arrive; p50 / p99 latency (submit to result) and
+    patches/s. The requests cycle through ``distinct`` seeded volumes of the
+    mix (a pool, so a long stream needs no volume generation on the clock);
+    the baseline is the same request list solved one after another host ->
+    host through ``denoise`` (each distinct volume timed once, warm)."""
     import torch
 
     from lowrank_gpu_fastest_b200 import api
     from lowrank_gpu_fastest_b200.harness import make_phantom_lowrank
+    from lowrank_gpu_fastest_b200.problem import n_patches
     from lowrank_gpu_fastest_b200.serve import Server, draw_request_shapes, poisson_arrivals
 
-    shapes = draw_request_shapes(args.requests, seed=args.seed, big_fraction=0.1)
-    arr = poisson_arrivals(args.rate, float("inf"), seed=args.seed, max_count=args.requests)
+    arr = poisson_arrivals(rate, duration if duration else float("inf"), seed=seed,
+                           max_count=None if duration else requests)
+    k = max(1, min(distinct, len(arr)))
+    shapes = draw_request_shapes(k, seed=seed, big_fraction=0.1)
     vols = [make_phantom_lowrank(r["shape"], seed=i, sigma=r["sigma"])[0] for i, r in enumerate(shapes)]
-    # warm: plans and one solve per distinct problem
-    seen = set()
-    for v, r in zip(vols, shapes):
-        k = (v.shape, r["patch"], r["stride"])
-        if k not in seen:
-            seen.add(k)
-            api.denoise(torch.from_numpy(v).cuda(), r["patch"], r["stride"])
-    torch.cuda.synchronize()
-    # sequential plain-form solves (host -> host each)
-    t0 = time.perf_counter()
-    for v, r in zip(vols, shapes):
+    seq = []
+    for v, r in zip(vols, shapes):  # warm plans, then one host -> host solve each
+        api.denoise(torch.from_numpy(v).cuda(), r["patch"], r["stride"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         api.denoise(v, r["patch"], r["stride"])
-    seq_s = time.perf_counter() - t0
-    from lowrank_gpu_fastest_b200.problem import n_patches
-
-    P = sum(n_patches(v.shape, r["patch"], r["stride"]) for v, r in zip(vols, shapes))
-    with Server(n_slots=4) as srv:
+        seq.append(time.perf_counter() - t0)
+    idx = [i % k for i in range(len(arr))]
+    P = sum(n_patches(vols[i].shape, shapes[i]["patch"], shapes[i]["stride"]) for i in idx)
+    seq_s = sum(seq[i] for i in idx)
+    with Server(n_slots=slots) as srv:
         start = time.perf_counter()
         futs = []
-        for t, v, r in zip(arr, vols, shapes):
+        for t, i in zip(arr, idx):
             now = time.perf_counter() - start
             if t > now:
                 time.sleep(t - now)
-            futs.append(srv.submit(v, r["patch"], r["stride"]))
+            futs.append(srv.submit(vols[i], shapes[i]["patch"], shapes[i]["stride"]))
         for f in futs:
             f.result()
         st = srv.stats()
-    print(json.dumps(dict(
-        metric="patches_per_s", workload="serving", value=st["patches_per_s"], unit="patches/s", n_gpus=1,
-        higher_is_better=True, dtype="f32", data="synthetic",
-        p50_ms=st["p50_ms"], p99_ms=st["p99_ms"], mean_ms=st["mean_ms"], requests=st["n"],
-        requests_per_s=st["requests_per_s"], sequential_patches_per_s=P / seq_s,
-        vs_sequential=st["patches_per_s"] / (P / seq_s),
-        config=dict(requests=args.requests, rate_per_s=args.rate, seed=args.seed, slots=4,
-                    mix="x,y 64..128, z 32..64, T {32,48,64,96}, patch {5,7,11}^3, stride {1,2,3}; "
-                        "10% 128x128x64x96 / 11^3 / stride 2"))), flush=True)
+    return dict(value=st["patches_per_s"], unit="patches/s", p50_ms=st["p50_ms"], p99_ms=st["p99_ms"],
+                mean_ms=st["mean_ms"], requests=st["n"], requests_per_s=st["requests_per_s"],
+                offered_rate_per_s=rate, duration_s=duration, span_s=st["span_s"],
+                sequential_patches_per_s=P / seq_s, vs_sequential=st["patches_per_s"] / (P / seq_s),
+                sequential_ms_per_request=1e3 * seq_s / max(1, len(idx)),
+                config=dict(requests=len(arr), rate_per_s=rate, seed=seed, slots=slots, distinct_volumes=k,
+                            mix="x,y 64..128, z 32..64, T {32,48,64,96}, patch {5,7,11}^3, stride {1,2,3}; "
+                                "10% 128x128x64x96 / 11^3 / stride 2"))
+
+
+def run_serving(args):
+    """``--workload serving``: ``--requests`` requests at ``--rate`` req/s, or
+    with ``--duration`` the stream of that many seconds (the serving
+    configuration: 40 req/s for 60 s)."""
+    r = serving_run(args.requests, args.rate, args.seed, duration=args.duration or None)
+    print(json.dumps(dict(metric="patches_per_s", workload="serving", n_gpus=1, higher_is_better=True, dtype="f32",
+                          data="synthetic", **r)), flush=True)
 
 
 def main():

@@ -96,6 +96,11 @@ struct lrd_plan {
   cudaStream_t io_prep[3] = {nullptr, nullptr, nullptr};  // centre + Gram of slab s on io_prep[s % 3]
   cudaStream_t io_recon = nullptr;                         // reconstruction of the slabs
   std::vector<cudaEvent_t> io_events;  // 5 per slab + 1
+  // device-resident pipeline of lrd_denoise: x-slabs whose Gram, solve and
+  // reconstruction overlap on the plan's streams (1 = one pass per phase);
+  // the enqueue of a call holds the mutex (the streams and events are shared)
+  int dev_slabs = 1;
+  mutable std::mutex pipe_mu;
   // measurement hook: a ring of per-call phase events
   bool profiling = false;
   int prof_calls = 0;
@@ -777,6 +782,14 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     }
   }
 
+  // device-resident pipeline: about one slab per 2048 patches, at most 8 (and
+  // LRD_DEVICE_SLABS overrides it, 1 = phases one after another)
+  {
+    long long sl = std::max<long long>(1, std::min<long long>(8, g.npatch / 2048));
+    if (const char* env = getenv("LRD_DEVICE_SLABS")) sl = std::max(1, atoi(env));
+    P->dev_slabs = (int)std::min<long long>({sl, (long long)g.ncx, (long long)kIoSlabs});
+  }
+
   // workspace layout
   size_t off = 0;
   P->off_mean = off; off += align256(sizeof(float) * (size_t)nvox);
@@ -886,6 +899,62 @@ int lrd_workspace_size(const lrd_plan* P, size_t* bytes) {
   return LRD_OK;
 }
 
+// lrd_denoise over x-slabs of patch corners whose phases overlap: slab s is
+// centred and its columns' Grams formed on a plan stream (io_prep[s % 3], after
+// the previous slab's centring, whose planes its columns share), its patches
+// solved and refined on ``st`` once its Grams are in, and the bricks whose
+// touching patches are then all final reconstructed on io_recon - so one
+// slab's latency-bound eigensolve shares the SMs with the next slab's Gram
+// and the previous slab's reconstruction. Every patch and voxel computes
+// exactly what the one-pass call computes (same kernels, same order per
+// voxel). All side streams join ``st`` again.
+int run_pipelined(const lrd_plan* P, const float* d_vol, float* d_out, char* ws, cudaStream_t st) {
+  const lrd::Geom& g = P->g;
+  const long long plane_vox = (long long)g.ny * g.nz;
+  float* gv = reinterpret_cast<float*>(ws + P->off_gv);
+  int32_t* rank = reinterpret_cast<int32_t*>(ws + P->off_rank);
+  float* wgt = reinterpret_cast<float*>(ws + P->off_wgt);
+  // k: 1 centred, 2 Gram, 3 reconstructed, 4 solved
+  auto ev = [&](int s, int k) { return P->io_events[5 * s + k]; };
+  cudaEvent_t start = P->io_events[5 * kIoSlabs];
+  int rc;
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 2 * sizeof(int32_t), st));
+  LRD_CUDA(cudaEventRecord(start, st));
+  for (auto ps : P->io_prep) LRD_CUDA(cudaStreamWaitEvent(ps, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
+  const int S = P->dev_slabs;
+  int planes_in = 0, ci_done = 0, bx_done = 0;
+  const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
+  for (int s = 0; s < S; ++s) {
+    const int ci_end = (int)((long long)(s + 1) * g.ncx / S);
+    const bool lastslab = s == S - 1;
+    const int x_need = lastslab ? g.nx : std::min(g.nx, P->h_corner_x[ci_end - 1] + g.px);
+    cudaStream_t prep = P->io_prep[s % 3];
+    if (s > 0) LRD_CUDA(cudaStreamWaitEvent(prep, ev(s - 1, 1), 0));
+    if (x_need > planes_in &&
+        (rc = run_center(P, d_vol, ws, prep, planes_in * plane_vox, (long long)(x_need - planes_in) * plane_vox)))
+      return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 1), prep));
+    planes_in = std::max(planes_in, x_need);
+    if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz))) return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
+    LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
+    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false))) return rc;
+    ci_done = ci_end;
+    int bx_end = bx_done;
+    while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
+    LRD_CUDA(cudaEventRecord(ev(s, 4), st));
+    LRD_CUDA(cudaStreamWaitEvent(P->io_recon, ev(s, 4), 0));
+    if ((rc = run_recon(P, ws, d_out, P->io_recon, bx_done * brz, bx_end * brz))) return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 3), P->io_recon));
+    bx_done = bx_end;
+  }
+  // the side streams join the caller's stream (every Gram event was waited on above)
+  LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 1, 3), 0));
+  return LRD_OK;
+}
+
 int lrd_denoise(const lrd_plan* P, const float* d_vol, float* d_out, int32_t* d_ranks, void* d_ws,
                 void* stream) {
   int rc = check_plan(P);
@@ -905,6 +974,12 @@ int lrd_denoise(const lrd_plan* P, const float* d_vol, float* d_out, int32_t* d_
   if (P->profiling && P->prof_calls < kProfRing) {
     ev = const_cast<cudaEvent_t*>(P->prof_events.data()) + (size_t)P->prof_calls * (LRD_NUM_PHASES + 1);
     ++const_cast<lrd_plan*>(P)->prof_calls;
+  }
+  if (!ev && P->dev_slabs > 1 && !P->is_slab) {
+    std::lock_guard<std::mutex> lk(P->pipe_mu);
+    if ((rc = run_pipelined(P, d_vol, d_out, ws, st))) return rc;
+    if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToDevice, st));
+    return LRD_OK;
   }
   if (ev) LRD_CUDA(cudaEventRecord(ev[0], st));
   LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
@@ -947,6 +1022,7 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   // planes back (copy-out stream). Events order: copy-in(s) -> centre(s)
   // (after centre(s - 1), whose planes the slab's columns share) -> Gram(s)
   // -> solve(s) -> reconstruct(s) -> copy-out(s).
+  std::lock_guard<std::mutex> lk(P->pipe_mu);  // the plan's streams and events
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   char* ws = static_cast<char*>(d_ws);
   const lrd::Geom& g = P->g;

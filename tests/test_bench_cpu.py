@@ -19,9 +19,10 @@ def test_phase_kernel_names():
     assert bench.phase_kernel("gram", 96, "tensor") == "gram_z_kernel"
     assert bench.phase_kernel("eigh_mp", 64, "plain") == "eigh_reg_kernel"
     assert bench.phase_kernel("eigh_mp", 96, "plain") == "eigh_cta_kernel"
-    assert bench.phase_kernel("recon", 48, "plain") == "recon_kernel_t24s2"
-    assert bench.phase_kernel("recon", 48, "accurate") == "recon_kernel"
-    assert bench.phase_kernel("recon", 64, "plain") == "recon_kernel"
+    assert bench.phase_kernel("recon", 48, "plain") == "recon_warp_kernel"
+    assert bench.phase_kernel("recon", 96, "accurate") == "recon_warp_kernel"
+    assert bench.phase_kernel("recon", 46, "plain") == "recon_kernel_t24s2"
+    assert bench.phase_kernel("recon", 80, "plain") == "recon_kernel"
 
 
 def test_roofline_arithmetic():

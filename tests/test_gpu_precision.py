@@ -63,7 +63,7 @@ def test_precision_forms_vs_fp64_headline(cuda_ok, rank, sigma):
     import torch
 
     vol = make_phantom_lowrank(HEADLINE, rank=rank, sigma=sigma, seed=3)[0]
-    ref64, _ = orc.denoise_fp64_parallel(vol, PATCH, STRIDE)
+    ref64, ranks64 = orc.denoise_fp64_parallel(vol, PATCH, STRIDE)
     ranks32 = orc.ranks_parallel(vol, PATCH, STRIDE)
     d = torch.from_numpy(vol).cuda()
     errs = {}
@@ -72,7 +72,13 @@ def test_precision_forms_vs_fp64_headline(cuda_ok, rank, sigma):
         out, ranks = api.denoise(d, PATCH, STRIDE, form=form, return_ranks=True)
         torch.cuda.synchronize()
         out, ranks = out.cpu().numpy(), ranks.cpu().numpy()
-        np.testing.assert_array_equal(ranks, ranks32)
+        # every rank equals step 0's, except where step 0's float32 decision differs
+        # from the float64 run's (a margin below step 0's own rounding): there the
+        # library's float64 near-tie pass takes the float64 decision
+        step0_off = ranks32 != ranks64
+        ok = (ranks == ranks32) | (step0_off & (ranks == ranks64))
+        assert ok.all(), f"{form}: {(~ok).sum()} ranks differ from step 0 and from the float64 run"
+        errs[f"{form}_ranks_at_step0_near_ties"] = int((ranks != ranks32).sum())
         errs[form] = rel_l2(out.astype(np.float64), ref64)
         outs[form] = out
     num = den = 0.0
