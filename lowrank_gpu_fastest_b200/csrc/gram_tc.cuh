@@ -224,10 +224,15 @@ __global__ void __launch_bounds__(kGramTcThreads)
     __syncthreads();  // H complete; the accumulator is free for plane zr + 2
     const int klo = max(tab.cover[2][2 * zr], wlo), khi = min(tab.cover[2][2 * zr + 1], whi);
     bool done_any = false;
+    const int slot0 = klo % ring;  // window k's slot is (slot0 + k - klo) mod ring
     for (int e = tid; e < ntri; e += nth) {
       const uint32_t rc = tri[e];
       const float h = H[(rc & 0xffff) * TH + (rc >> 16)];
-      for (int k = klo; k <= khi; ++k) win[(size_t)(k % ring) * ntri + e] += h;
+      int slot = slot0;
+      for (int k = klo; k <= khi; ++k) {
+        win[(size_t)slot * ntri + e] += h;
+        if (++slot == ring) slot = 0;
+      }
     }
     for (int k = klo; k <= khi; ++k) done_any |= zr == tab.corners[2][k] + g.pz - 1;
     if (done_any) {  // uniform
@@ -265,8 +270,14 @@ __global__ void __launch_bounds__(kGramTcThreads)
     const float* pl = planes + (size_t)s * pf;
     unsigned char* hi = smt + (size_t)s * 2 * tile;
     unsigned char* lo = hi + tile;
-    for (int e = tid; e < T * nv4; e += nth) {
-      const int v4 = e / T, t = e - v4 * T;
+    // item e = v4 * T + t, stepped by nth without a division per step
+    const int dq = nth / T, dr = nth - (nth / T) * T;
+    int v4 = tid / T, t = tid - (tid / T) * T;
+    for (int e = tid; e < T * nv4; e += nth, v4 += dq, t += dr) {
+      if (t >= T) {
+        t -= T;
+        ++v4;
+      }
       uint32_t hh[4], ll[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {

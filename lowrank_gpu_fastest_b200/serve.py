@@ -12,8 +12,10 @@ owns the device:
   pinned staging buffer, ``lrd_denoise``, device->host copy into pinned
   memory, an event; requests on different slots overlap on the device;
 * completion - the scheduler polls the events without blocking, resolves the
-  future with the denoised volume (and ranks), frees the slot and the
-  request's device buffers, and admits the next requests.
+  future with the denoised volume (and ranks), frees the slot, returns the
+  request's device buffers to a pool (reused by later requests of the same
+  size class, so a steady stream allocates no device memory after warm-up)
+  and admits the next requests.
 
 Because every kernel is deterministic and a request's arithmetic does not
 depend on what runs beside it, a request's result is bit-identical alone and
@@ -49,6 +51,42 @@ class _Req:
     t_start: float = 0.0
 
 
+class _Pool:
+    """Buffers kept for reuse across requests, by kind and size class: a
+    request takes the smallest free buffer of its kind that is large enough
+    (sizes rounded up to 2 MiB classes) and gives it back when it completes,
+    so a steady stream allocates nothing after warm-up."""
+
+    CLASS = 2 << 20
+
+    def __init__(self, alloc):
+        self.alloc = alloc  # (kind, nbytes) -> uint8 tensor of nbytes
+        self.free: dict = collections.defaultdict(list)
+        self.free_bytes = 0
+
+    def take(self, kind, nbytes):
+        nb = max(self.CLASS, -(-int(nbytes) // self.CLASS) * self.CLASS)
+        lst = self.free[kind]
+        best = None
+        for i, t in enumerate(lst):
+            if t.numel() >= nb and (best is None or t.numel() < lst[best].numel()):
+                best = i
+        if best is not None:
+            t = lst.pop(best)
+            self.free_bytes -= t.numel()
+            return t
+        return self.alloc(kind, nb)
+
+    def give(self, kind, t):
+        self.free[kind].append(t)
+        self.free_bytes += t.numel()
+
+    def trim(self):
+        """Drop every free buffer (the device memory returns to the allocator)."""
+        self.free.clear()
+        self.free_bytes = 0
+
+
 class Server:
     """Continuous-batching denoise server on one CUDA device."""
 
@@ -73,6 +111,11 @@ class Server:
         with torch.cuda.device(device):
             self._streams = [torch.cuda.Stream(device=device) for _ in range(self.n_slots)]
         self._free_slots = list(range(self.n_slots))
+
+        def alloc(kind, nbytes):
+            return torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{device}")
+
+        self._pool = _Pool(alloc)
 
     # -- public --------------------------------------------------------------
     def start(self):
@@ -152,7 +195,15 @@ class Server:
 
     def _fits(self, need):
         free, _ = self.torch.cuda.mem_get_info(self.device)
-        if need > free - self.reserve:
+        # pooled device buffers are reused first; torch's cache is reusable too
+        cached = self.torch.cuda.memory_reserved(self.device) - self.torch.cuda.memory_allocated(self.device)
+        avail = free + cached + self._pool.free_bytes - self.reserve
+        if need > avail and self._pool.free_bytes:
+            self._pool.trim()  # give the pooled buffers back before refusing
+            self.torch.cuda.empty_cache()
+            free, _ = self.torch.cuda.mem_get_info(self.device)
+            avail = free - self.reserve
+        if need > avail:
             return False
         if self.budget is not None and self._in_flight_bytes + need > self.budget:
             return False
@@ -183,20 +234,23 @@ class Server:
             dev = f"cuda:{self.device}"
             with torch.cuda.device(self.device), torch.cuda.stream(st):
                 h_in = r.h_in
-                d_in = torch.empty(r.vol.shape, dtype=torch.float32, device=dev)
-                d_out = torch.empty_like(d_in)
-                d_rank = torch.empty(r.n_patches, dtype=torch.int32, device=dev)
-                ws = torch.empty(max(plan.workspace_bytes, 1), dtype=torch.uint8, device=dev)
-                d_in.copy_(h_in, non_blocking=True)
-                plan.denoise(d_in.data_ptr(), d_out.data_ptr(), d_rank.data_ptr(), ws.data_ptr(), st.cuda_stream)
+                vbytes, rbytes = r.vol.nbytes, 4 * r.n_patches
+                raw = {k: self._pool.take(k, n) for k, n in (("d_in", vbytes), ("d_out", vbytes),
+                                                           ("d_rank", rbytes), ("ws", max(plan.workspace_bytes, 1)))}
+                d_in = raw["d_in"][:vbytes].view(torch.float32).view(r.vol.shape)
+                d_out = raw["d_out"][:vbytes].view(torch.float32).view(r.vol.shape)
+                d_rank = raw["d_rank"][:rbytes].view(torch.int32)
+                # the result's pinned buffers go to the caller (torch's host allocator caches them)
                 h_out = torch.empty(r.vol.shape, dtype=torch.float32, pin_memory=True)
                 h_rank = torch.empty(r.n_patches, dtype=torch.int32, pin_memory=True)
+                d_in.copy_(h_in, non_blocking=True)
+                plan.denoise(d_in.data_ptr(), d_out.data_ptr(), d_rank.data_ptr(), raw["ws"].data_ptr(),
+                             st.cuda_stream)
                 h_out.copy_(d_out, non_blocking=True)
                 h_rank.copy_(d_rank, non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(st)
-            r.bufs = dict(h_in=h_in, d_in=d_in, d_out=d_out, d_rank=d_rank, ws=ws, h_out=h_out, h_rank=h_rank,
-                          plan=plan)
+            r.bufs = dict(h_in=h_in, raw=raw, h_out=h_out, h_rank=h_rank, plan=plan)
             r.event = ev
             self._running[id(r)] = r
 
@@ -209,6 +263,8 @@ class Server:
             t_done = time.perf_counter()
             out = r.bufs["h_out"].numpy()
             ranks = r.bufs["h_rank"].numpy()
+            for k, t in r.bufs["raw"].items():
+                self._pool.give(k, t)
             r.bufs = {}
             r.h_in = None
             self._free_slots.append(r.slot)
