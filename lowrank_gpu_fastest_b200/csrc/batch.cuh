@@ -121,7 +121,7 @@ __global__ void eigh_refine_batch_kernel(const BatchVol* __restrict__ vols, cons
                                          const long long* __restrict__ off, int n) {
   const int i = batch_find(off, n, blockIdx.x);
   const BatchVol& V = vols[list[i]];
-  eigh_refine_body(V.xc, V.gv, nullptr, V.rank, V.wgt, V.sig2, V.g, V.tab, V.refine, V.refine + 64,
+  eigh_refine_body(V.vol, V.xc, V.gv, nullptr, V.rank, V.wgt, V.sig2, V.g, V.tab, V.refine, V.refine + 64,
                    (int)(blockIdx.x - off[i]), (int)(off[i + 1] - off[i]));
 }
 

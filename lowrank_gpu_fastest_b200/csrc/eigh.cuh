@@ -26,10 +26,11 @@
 // in float32 on the float32 Gram. A patch whose MP test has an index with
 // |lhs/rhs - 1| below kRefineTol (a near-tie that float32 round-off could
 // decide either way) is queued, and eigh_refine_kernel redoes it in float64:
-// the Gram from exact float64 products of the float32 centred data with a
+// each voxel's time course centred in float64 from the input volume (the
+// float64 mean of its float32 values), the Gram from float64 products with a
 // float64 sum, then the same eigen/MP/eigenvector steps in float64 - so
 // near-ties are decided as the float64 evaluation of the algorithm decides
-// them.
+// them, down to margins far below the float32 centred data's own rounding.
 //
 // Output per patch: the p eigenvectors (descending eigenvalue order) as the
 // rows of a compact p x T block at the start of the patch's T x T slot (the
@@ -532,7 +533,10 @@ constexpr int kRefinePrefetch = 16; // floats of the next z-run a thread prefetc
 // holds a handful of patches per volume, so this pass is one patch's latency:
 // every step of it is spread over the block.
 // Body: this block is block ``bid`` of ``nblocks`` working on one volume's queue.
-__device__ __forceinline__ void eigh_refine_body(const float* __restrict__ xc, float* vecs,
+// ``vol`` (nullable): the input volume - its voxel rows are centred here in
+// float64; without it the float32 centred rows ``xc`` are used as they are.
+__device__ __forceinline__ void eigh_refine_body(const float* __restrict__ vol, const float* __restrict__ xc,
+                                                 float* vecs,
                                                  float* __restrict__ lam_out, int32_t* __restrict__ ranks,
                                                  float* __restrict__ wgt, float* __restrict__ sig2, const Geom& g,
                                                  const AxisTables& tab, const int* __restrict__ refine_count,
@@ -558,7 +562,21 @@ __device__ __forceinline__ void eigh_refine_body(const float* __restrict__ xc, f
     int ci, cj, ck;
     patch_axes(g, pid, ci, cj, ck);
     const int cx = tab.corners[0][ci], cy = tab.corners[1][cj], cz = tab.corners[2][ck];
-    auto run_src = [&](int q) { return xc + voxel_row(g, cx + q / g.py, cy + q % g.py, cz) * n; };
+    const float* src0 = vol != nullptr ? vol : xc;
+    auto run_src = [&](int q) { return src0 + voxel_row(g, cx + q / g.py, cy + q % g.py, cz) * n; };
+    // the staged run's voxel rows centred in float64 (float32 input values are
+    // exact in float64; the mean is their float64 sum / T)
+    auto centre_run = [&](double* run) {
+      if (vol == nullptr) return;
+      __syncthreads();
+      for (int r = tid; r < g.pz; r += nth) {
+        double* row = run + (size_t)r * n;
+        double sum = 0.0;
+        for (int t = 0; t < n; ++t) sum += row[t];
+        const double m = sum / n;
+        for (int t = 0; t < n; ++t) row[t] -= m;
+      }
+    };
     // G = Xc^T Xc in float64 (products of float32 values are exact in float64);
     // entry (r, c), r <= c, sums over the runs in x-major voxel order
     for (int base = 0; base < nent; base += kRefineEntries * nth) {
@@ -583,6 +601,7 @@ __device__ __forceinline__ void eigh_refine_body(const float* __restrict__ xc, f
         const float* src = run_src(0);
         for (int e = tid; e < runlen; e += nth) runs[e] = (double)src[e];
       }
+      centre_run(runs);
       __syncthreads();
       for (int q = 0; q < nruns; ++q) {
         const double* cur = runs + (size_t)(q & 1) * runlen;
@@ -616,6 +635,7 @@ __device__ __forceinline__ void eigh_refine_body(const float* __restrict__ xc, f
             const float* src = run_src(q + 1);
             for (int e = tid; e < runlen; e += nth) nxt[e] = (double)src[e];
           }
+          centre_run(nxt);
         }
         __syncthreads();
       }
@@ -635,11 +655,12 @@ __device__ __forceinline__ void eigh_refine_body(const float* __restrict__ xc, f
   }
 }
 
-__global__ void eigh_refine_kernel(const float* __restrict__ xc, float* vecs, float* __restrict__ lam_out,
+__global__ void eigh_refine_kernel(const float* __restrict__ vol, const float* __restrict__ xc, float* vecs,
+                                   float* __restrict__ lam_out,
                                    int32_t* __restrict__ ranks, float* __restrict__ wgt, float* __restrict__ sig2,
                                    Geom g, AxisTables tab, const int* __restrict__ refine_count,
                                    const int* __restrict__ refine_ids) {
-  eigh_refine_body(xc, vecs, lam_out, ranks, wgt, sig2, g, tab, refine_count, refine_ids, (int)blockIdx.x,
+  eigh_refine_body(vol, xc, vecs, lam_out, ranks, wgt, sig2, g, tab, refine_count, refine_ids, (int)blockIdx.x,
                    (int)gridDim.x);
 }
 

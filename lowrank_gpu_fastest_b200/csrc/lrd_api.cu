@@ -432,7 +432,8 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
 // [count, refined, 62 unused, ids...]; the centred volume there is the one
 // the Gram was formed from). ``reset`` clears the queue first.
 int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, float* d_lam, int32_t* d_rank,
-             float* d_wgt, cudaStream_t st, long long p_lo = 0, long long p_hi = -1, bool reset = true) {
+             float* d_wgt, cudaStream_t st, long long p_lo = 0, long long p_hi = -1, bool reset = true,
+             const float* d_vol = nullptr) {
   const long long npatch = P->g.npatch;
   if (p_hi < 0) p_hi = npatch;
   const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
@@ -470,7 +471,8 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
     if (rc) return rc;
   }
   const float* xc = reinterpret_cast<const float*>(ws + P->off_xc);
-  lrd::eigh_refine_kernel<<<P->refine_blocks, 128, P->smem_refine, st>>>(xc, d_vecs, d_lam, d_rank, d_wgt, sig2,
+  lrd::eigh_refine_kernel<<<P->refine_blocks, 128, P->smem_refine, st>>>(d_vol, xc, d_vecs, d_lam, d_rank, d_wgt,
+                                                                        sig2,
                                                                         P->g, P->tab, rcount, rids);
   int rc = launch_check("eigh_refine_kernel launch");
   if (rc) return rc;
@@ -782,10 +784,16 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     }
   }
 
-  // device-resident pipeline: about one slab per 2048 patches, at most 8 (and
-  // LRD_DEVICE_SLABS overrides it, 1 = phases one after another)
+  // device-resident pipeline: off by default (LRD_DEVICE_SLABS = S > 1 turns it
+  // on). Measured on B200, device ms per denoise at 96x96x48x48 / 11^3 /
+  // stride 3, plain, S = 1 / 2 / 3 / 4 / 6 / 8 / 12: 2.86 / 2.94 / 2.94 / 2.93 /
+  // 2.95 / 3.19 / 3.42 (accurate 3.13 -> 3.21 .. 3.57): a slab's eigensolve
+  // takes one matrix's latency (~0.2 ms) however few matrices it has, and
+  // the eigensolver's CTAs leave little room on the SMs for the neighbouring
+  // slabs' Gram and reconstruction, so the phases do not overlap enough to
+  // pay for the extra launches.
   {
-    long long sl = std::max<long long>(1, std::min<long long>(8, g.npatch / 2048));
+    long long sl = 1;
     if (const char* env = getenv("LRD_DEVICE_SLABS")) sl = std::max(1, atoi(env));
     P->dev_slabs = (int)std::min<long long>({sl, (long long)g.ncx, (long long)kIoSlabs});
   }
@@ -940,7 +948,8 @@ int run_pipelined(const lrd_plan* P, const float* d_vol, float* d_out, char* ws,
     if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
     LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
-    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false))) return rc;
+    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false, d_vol)))
+      return rc;
     ci_done = ci_end;
     int bx_end = bx_done;
     while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
@@ -987,7 +996,7 @@ int lrd_denoise(const lrd_plan* P, const float* d_vol, float* d_out, int32_t* d_
   if (ev) LRD_CUDA(cudaEventRecord(ev[1], st));
   if ((rc = run_gram(P, ws, gv, st))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[2], st));
-  if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st))) return rc;
+  if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, 0, -1, true, d_vol))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[3], st));
   if ((rc = run_recon(P, ws, d_out, st))) return rc;
   if (ev) LRD_CUDA(cudaEventRecord(ev[4], st));
@@ -1066,7 +1075,7 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
     if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz, s == 0))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
     LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
-    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false))) return rc;
+    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false, d_in))) return rc;
     ci_done = ci_end;
     int bx_end = bx_done;
     while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
@@ -1158,7 +1167,7 @@ int lrd_slab_prepare(const lrd_plan* P, const float* d_vol, int32_t* d_ranks, vo
   LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
   if ((rc = run_center(P, d_vol, ws, st))) return rc;
   if ((rc = run_gram(P, ws, gv, st))) return rc;
-  if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st))) return rc;
+  if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, 0, -1, true, d_vol))) return rc;
   if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * P->g.npatch, cudaMemcpyDeviceToDevice, st));
   return LRD_OK;
 }
