@@ -106,6 +106,10 @@ __host__ __device__ constexpr size_t eigh_hv_floats() {
 }
 constexpr int kLdy = kInvGroup + 1;  // eigenvector chunk row stride
 constexpr double kRefineTol = 1e-4;  // MP-test margin below which float64 redoes the patch
+// Margin of the float64 pass's step-0 emulation below which its decision is
+// taken from the test in float64 throughout (within float32 resolution of the
+// data, step 0's float32 arithmetic could decide either way).
+constexpr double kTieFloor = 1e-6;
 
 __host__ __device__ inline int eigh_lda(int n) { return n + ((n & 1) ? 2 : 1); }
 
@@ -118,7 +122,8 @@ __host__ __device__ inline size_t eigh_smem_elems(int n) {
 
 // MP rank from the ascending eigenvalues lam * unscale, evaluated like
 // step0_numpy_loop.py:18-24 (float32 eigs and suffix sums, float64 test,
-// a count over all indices); W holds 2n floats of scratch. Returns the
+// a count over all indices); W holds 2n floats of scratch (4n + 2 in the
+// float64 instantiation, whose W is 8-byte aligned). Returns the
 // smallest |lhs/rhs - 1| over the indices. With ``sig2_out`` lane 0 also
 // writes the patch's noise variance estimate, the mean of the t - p noise
 // eigenvalues: rcum_p / (t - p) in float32 (0 when p = t). One warp.
@@ -161,6 +166,32 @@ __device__ double mp_rank(const Real* lam, Real unscale, int n, int nvox, float*
       p += __popc(__ballot_sync(0xffffffffu, sig));
     }
     margin = warp_min(margin);
+  }
+  if constexpr (sizeof(Real) == 8) {
+    // The float64 near-tie pass. Below a margin of kTieFloor the step-0
+    // emulation (float32 eigs and sums) decides within float32 resolution of
+    // the data - step 0's own float32 SVD could land either way - so the
+    // count is taken from the test in float64 throughout (eigs, suffix sums
+    // and products), the decision of the float64 run of the algorithm.
+    if (margin < kTieFloor) {
+      double* e64 = reinterpret_cast<double*>(rc + n);  // past the float32 arrays (float offset 2n: 8-byte aligned)
+      for (int i = lane; i < t; i += 32) e64[i] = fmax((double)lam[n - 1 - i] * (double)unscale, 0.0) / nvox;
+      __syncwarp();
+      double r64 = 0.0, tail = 0.0;
+      const double sq = sqrt((double)((long long)t * (long long)nvox));
+      int p64 = 0;
+      // suffix sums in double by lane 0 (t <= 127 terms), then the count
+      if (lane == 0) {
+        for (int i = t - 1; i >= 0; --i) {
+          r64 += e64[i];
+          const double lhs = (e64[i] - e64[t - 1]) * (double)(t - i) * (double)(nvox - i);
+          p64 += lhs > 4.0 * r64 * sq;
+        }
+        tail = (double)p64;
+      }
+      p = (int)__shfl_sync(0xffffffffu, tail, 0);
+      __syncwarp();
+    }
   }
   p_out = p;
   if (sig2_out != nullptr && lane == 0) *sig2_out = (p < t) ? __fdiv_rn(rc[p], (float)(t - p)) : 0.f;

@@ -95,6 +95,7 @@ struct lrd_plan {
   cudaStream_t io_in = nullptr, io_out = nullptr;
   cudaStream_t io_prep[3] = {nullptr, nullptr, nullptr};  // centre + Gram of slab s on io_prep[s % 3]
   cudaStream_t io_recon = nullptr;                         // reconstruction of the slabs
+  cudaStream_t io_solve = nullptr;                         // solves of odd slabs (even ones: the caller's)
   std::vector<cudaEvent_t> io_events;  // 5 per slab + 1
   // device-resident pipeline of lrd_denoise: x-slabs whose Gram, solve and
   // reconstruction overlap on the plan's streams (1 = one pass per phase);
@@ -433,7 +434,7 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
 // the Gram was formed from). ``reset`` clears the queue first.
 int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, float* d_lam, int32_t* d_rank,
              float* d_wgt, cudaStream_t st, long long p_lo = 0, long long p_hi = -1, bool reset = true,
-             const float* d_vol = nullptr) {
+             const float* d_vol = nullptr, int queue = -1) {
   const long long npatch = P->g.npatch;
   if (p_hi < 0) p_hi = npatch;
   const long long batch = P->prob.batch > 0 ? P->prob.batch : npatch;
@@ -441,6 +442,13 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
   const long long TT = (long long)T * T;
   int* rcount = reinterpret_cast<int*>(ws + P->off_refine);
   int* rids = rcount + 64;
+  if (queue >= 0) {
+    // a private near-tie queue for patches [p_lo, p_hi): its counters at header
+    // ints 2 + 2q, 3 + 2q (zeroed by the caller), its ids where those patches'
+    // would go, so solves of different patch ranges can run at the same time
+    rcount += 2 + 2 * queue;
+    rids += p_lo;
+  }
   float* sig2 = reinterpret_cast<float*>(ws + P->off_sig2);
   if (reset) LRD_CUDA(cudaMemsetAsync(rcount, 0, 2 * sizeof(int), st));
   for (long long p0 = p_lo; p0 < p_hi; p0 += batch) {
@@ -762,7 +770,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   {
     cudaError_t e1 = cudaStreamCreateWithFlags(&P->io_in, cudaStreamNonBlocking);
     cudaError_t e2 = cudaStreamCreateWithFlags(&P->io_out, cudaStreamNonBlocking);
-    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_recon}) {
+    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_recon, &P->io_solve}) {
       cudaError_t e4 = cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking);
       if (e4 != cudaSuccess) {
         *ps = nullptr;
@@ -890,6 +898,7 @@ int lrd_plan_destroy(lrd_plan* P) {
   for (auto ps : P->io_prep)
     if (ps) cudaStreamDestroy(ps);
   if (P->io_recon) cudaStreamDestroy(P->io_recon);
+  if (P->io_solve) cudaStreamDestroy(P->io_solve);
   if (P->d_tables) cudaFree(P->d_tables);
   delete P;
   return LRD_OK;
@@ -927,10 +936,11 @@ int run_pipelined(const lrd_plan* P, const float* d_vol, float* d_out, char* ws,
   cudaEvent_t start = P->io_events[5 * kIoSlabs];
   int rc;
   LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
-  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 2 * sizeof(int32_t), st));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 64 * sizeof(int32_t), st));  // every slab's queue
   LRD_CUDA(cudaEventRecord(start, st));
   for (auto ps : P->io_prep) LRD_CUDA(cudaStreamWaitEvent(ps, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_solve, start, 0));
   const int S = P->dev_slabs;
   int planes_in = 0, ci_done = 0, bx_done = 0;
   const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
@@ -947,20 +957,25 @@ int run_pipelined(const lrd_plan* P, const float* d_vol, float* d_out, char* ws,
     planes_in = std::max(planes_in, x_need);
     if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
-    LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
-    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false, d_vol)))
+    // successive slabs' solves on two streams: one slab's solve takes a matrix's
+    // latency however few matrices it has, so two run side by side
+    cudaStream_t solve = (s & 1) ? P->io_solve : st;
+    LRD_CUDA(cudaStreamWaitEvent(solve, ev(s, 2), 0));
+    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, solve, ci_done * patz, ci_end * patz, false, d_vol, s)))
       return rc;
     ci_done = ci_end;
     int bx_end = bx_done;
     while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
-    LRD_CUDA(cudaEventRecord(ev(s, 4), st));
+    LRD_CUDA(cudaEventRecord(ev(s, 4), solve));
     LRD_CUDA(cudaStreamWaitEvent(P->io_recon, ev(s, 4), 0));
     if ((rc = run_recon(P, ws, d_out, P->io_recon, bx_done * brz, bx_end * brz))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 3), P->io_recon));
     bx_done = bx_end;
   }
-  // the side streams join the caller's stream (every Gram event was waited on above)
+  // the side streams join the caller's stream: the last reconstruction follows
+  // every solve (each reconstruction waited for its slab's) and every Gram
   LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 1, 3), 0));
+  for (int s = 0; s < S && s < 3; ++s) LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 1 - s, 2), 0));
   return LRD_OK;
 }
 
@@ -1044,12 +1059,13 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   auto ev = [&](int s, int k) { return P->io_events[5 * s + k]; };
   cudaEvent_t start = P->io_events[5 * kIoSlabs];
   LRD_CUDA(cudaMemsetAsync(ws + P->off_status, 0, sizeof(int32_t), st));
-  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 2 * sizeof(int32_t), st));
+  LRD_CUDA(cudaMemsetAsync(ws + P->off_refine, 0, 64 * sizeof(int32_t), st));  // every slab's queue
   LRD_CUDA(cudaEventRecord(start, st));
   LRD_CUDA(cudaStreamWaitEvent(P->io_in, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_out, start, 0));
   for (auto ps : P->io_prep) LRD_CUDA(cudaStreamWaitEvent(ps, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_solve, start, 0));
   // about 8 MiB of input per slab, at most kIoSlabsUsed slabs: a small volume's
   // slabs would be launch- and event-bound
   const long long vbytes = (long long)sizeof(float) * P->nvox * g.nt;
@@ -1074,12 +1090,16 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
     planes_in = std::max(planes_in, x_need);
     if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz, s == 0))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
-    LRD_CUDA(cudaStreamWaitEvent(st, ev(s, 2), 0));
-    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, st, ci_done * patz, ci_end * patz, false, d_in))) return rc;
+    // successive slabs' solves on two streams, each slab with its own near-tie
+    // queue: a slab's solve takes a matrix's latency however few it holds
+    cudaStream_t solve = (s & 1) ? P->io_solve : st;
+    LRD_CUDA(cudaStreamWaitEvent(solve, ev(s, 2), 0));
+    if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, solve, ci_done * patz, ci_end * patz, false, d_in, s)))
+      return rc;
     ci_done = ci_end;
     int bx_end = bx_done;
     while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
-    LRD_CUDA(cudaEventRecord(ev(s, 4), st));
+    LRD_CUDA(cudaEventRecord(ev(s, 4), solve));
     LRD_CUDA(cudaStreamWaitEvent(P->io_recon, ev(s, 4), 0));
     if ((rc = run_recon(P, ws, d_out, P->io_recon, bx_done * brz, bx_end * brz))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 3), P->io_recon));
