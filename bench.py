@@ -136,9 +136,11 @@ def phase_kernel(phase, T, form):
     """Kernel that a plan phase launches for T frames (the eigensolve phase
     also runs the refine kernel and its cursor, both under 0.5% of it)."""
     if phase == "gram":
-        return "gram_tc_kernel" if (form == "tensor" and T <= 64) else "gram_z_kernel"
+        return "gram_tc_kernel" if (form in ("tensor", "tensor_bf16") and T <= 64) else "gram_z_kernel"
     if phase == "eigh_mp":
         return "eigh_reg_kernel" if T <= 64 else "eigh_cta_kernel"
+    if phase == "recon" and form in ("tensor", "tensor_bf16") and T % 4 == 0 and 8 <= T <= 64:
+        return "recon_tc_kernel"  # tcgen05, 4x4x8 voxel bricks
     if phase == "recon" and T in (32, 48, 64, 96):
         return "recon_warp_kernel"  # one warp per 2x2x2 voxel block (the plan's default layout)
     if phase == "recon" and form == "plain" and 45 <= T <= 48:
@@ -152,7 +154,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--form", choices=["plain", "accurate", "tensor"], default="plain")
+    ap.add_argument("--form", choices=["plain", "accurate", "tensor", "tensor_bf16"], default="plain")
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batched", "serving"], default="headline")
     ap.add_argument("--volumes", type=int, default=24, help="batched: number of volumes")
     ap.add_argument("--requests", type=int, default=48, help="serving: number of requests")
@@ -803,11 +805,12 @@ def executed_fp32(ph, shape, patch, stride, ranks, fp32_peak, form):
     recon_fl = float(4 * T * N * np.asarray(ranks, dtype=np.float64).sum())
     out = dict(executed_gflop_gram=gram_fl / 1e9, executed_gflop_recon=recon_fl / 1e9,
                mean_rank=float(np.mean(ranks)))
-    if form != "tensor" or T > 64:
+    if form not in ("tensor", "tensor_bf16") or T > 64:
         out["executed_tflops_gram"] = gram_fl / (ph["gram"] * 1e-3) / 1e12
         out["gram_frac_of_sgemm"] = out["executed_tflops_gram"] / fp32_peak
-    out["executed_tflops_recon"] = recon_fl / (ph["recon"] * 1e-3) / 1e12
-    out["recon_frac_of_sgemm"] = out["executed_tflops_recon"] / fp32_peak
+    if phase_kernel("recon", T, form) != "recon_tc_kernel":
+        out["executed_tflops_recon"] = recon_fl / (ph["recon"] * 1e-3) / 1e12
+        out["recon_frac_of_sgemm"] = out["executed_tflops_recon"] / fp32_peak
     return out
 
 

@@ -65,7 +65,12 @@ enum lrd_form {
    * accumulation in tensor memory per plane (T <= 64, px*py <= 128; otherwise
    * the FP32 Gram), near-tie MP decisions redone in FP64, the accurate
    * form's accumulation. */
-  LRD_FORM_TENSOR = 2
+  LRD_FORM_TENSOR = 2,
+  /* Precision form with BF16 operands: as LRD_FORM_TENSOR, the Gram on
+   * tcgen05 in kind::f16 with each float32 value split into three BF16 terms
+   * (x = b0 + b1 + b2) and the six products of combined order <= 2 summed in
+   * FP32 in tensor memory per plane. */
+  LRD_FORM_TENSOR_BF16 = 3
 };
 
 /* One problem: volume (nx, ny, nz, nt), patch (px, py, pz), one stride for the

@@ -21,7 +21,7 @@ LRD_ERR_UNSUPPORTED = -4
 LRD_ERR_NODEVICE = -5
 LRD_ERR_TIMEOUT = -6
 
-FORMS = {"plain": 0, "accurate": 1, "tensor": 2}
+FORMS = {"plain": 0, "accurate": 1, "tensor": 2, "tensor_bf16": 3}
 
 # Every symbol include/lrd.h declares, with (restype, argtypes).
 _c_i32p = ctypes.POINTER(ctypes.c_int32)

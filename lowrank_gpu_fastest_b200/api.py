@@ -68,8 +68,9 @@ def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", retu
     (common.py:29), ``batch`` = patches per Gram/eigensolver launch
     (step8_tuned.py:21; ``None`` = all). ``form`` is ``"plain"`` (float32,
     step-0 accumulation order), ``"accurate"`` (float64 accumulation, close
-    to the float64 run) or ``"tensor"`` (as accurate, the Gram on the tensor
-    cores in split TF32). With ``return_ranks`` the per-patch MP ranks
+    to the float64 run), ``"tensor"`` (as accurate, the Gram on the tensor
+    cores in split TF32) or ``"tensor_bf16"`` (as tensor, with three-term
+    BF16 split products). With ``return_ranks`` the per-patch MP ranks
     (x-major patch order) are returned too. ``out`` (CUDA input only): a
     preallocated output tensor of the volume's shape.
     """

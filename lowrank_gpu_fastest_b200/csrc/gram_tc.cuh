@@ -27,7 +27,17 @@
 // waits (with the same bound) for the copies and MMAs it still has in flight,
 // and only then is the TMEM allocation released and the CTA retired; the
 // status word records the timeout.
+//
+// A second operand kind, kind::f16 with BF16 operands (the BF16 form): x is
+// split into three BF16 terms, x = b0 + b1 + b2 (b0 = bf16(x), b1 = bf16(x -
+// b0), b2 = bf16(x - b0 - b1): 24 bits of the float32 value), and
+//     H = b0.b0 + b0.b1 + b1.b0 + b0.b2 + b1.b1 + b2.b0
+// (every product of combined order <= 2; the dropped terms are below 2^-24
+// of the leading one), K = 16 voxels per instruction, FP32 accumulation in
+// TMEM as above.
 #pragma once
+
+#include <cuda_bf16.h>
 
 #include "gram_z.cuh"
 
@@ -55,6 +65,22 @@ __device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t smem_addr, uint32_
 __host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
+
+// Instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ uint32_t bf16_bits(float x) { return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float bf16_value(uint32_t b) { return __uint_as_float(b << 16); }
 
 __device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   asm volatile(
@@ -97,16 +123,32 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 // (M = 64); rows past T read whatever follows (the lo tile, or the plane
 // slots after the last tile) and only feed accumulator rows >= T, which are
 // never read back.
-__host__ __device__ inline int gramtc_kpad(int rows) { return (rows + 7) & ~7; }
-__host__ __device__ inline size_t gramtc_sbo(int rows) { return (size_t)(gramtc_kpad(rows) / 4) * 128; }
-__host__ __device__ inline size_t gramtc_tile_bytes(int rows, int T) { return (size_t)((T + 7) / 8) * gramtc_sbo(rows); }
-__host__ __device__ inline size_t gramtc_off_plane(int rows, int T) { return 4 * gramtc_tile_bytes(rows, T); }
+// Operand layout per kind: a core matrix row holds 16 bytes = 4 TF32 or 8
+// BF16 values along K; an instruction's K (8 TF32, 16 BF16) spans two core
+// matrices; a stage holds 2 (hi, lo) or 3 (b0, b1, b2) split tiles.
+__host__ __device__ inline int gramtc_kvals(bool bf16) { return bf16 ? 8 : 4; }
+__host__ __device__ inline int gramtc_parts(bool bf16) { return bf16 ? 3 : 2; }
+__host__ __device__ inline int gramtc_kpad(int rows, bool bf16 = false) {
+  const int k = 2 * gramtc_kvals(bf16);
+  return (rows + k - 1) / k * k;
+}
+__host__ __device__ inline size_t gramtc_sbo(int rows, bool bf16 = false) {
+  return (size_t)(gramtc_kpad(rows, bf16) / gramtc_kvals(bf16)) * 128;
+}
+__host__ __device__ inline size_t gramtc_tile_bytes(int rows, int T, bool bf16 = false) {
+  return (size_t)((T + 7) / 8) * gramtc_sbo(rows, bf16);
+}
+__host__ __device__ inline size_t gramtc_off_plane(int rows, int T, bool bf16 = false) {
+  return 2 * (size_t)gramtc_parts(bf16) * gramtc_tile_bytes(rows, T, bf16);
+}
 __host__ __device__ inline int gramtc_ntri(int T) { return T * (T + 1) / 2; }
-__host__ __device__ inline size_t gramtc_smem_bytes(int rows, int T, int ring) {
+__host__ __device__ inline size_t gramtc_smem_bytes(int rows, int T, int ring, bool bf16 = false) {
   const size_t planes = 2 * sizeof(float) * gramz_plane_floats(rows, T);
-  const size_t end = gramtc_off_plane(rows, T) + planes + sizeof(float) * (size_t)T * (T + 1) +
+  const size_t end = gramtc_off_plane(rows, T, bf16) + planes + sizeof(float) * (size_t)T * (T + 1) +
                      sizeof(float) * (size_t)ring * gramtc_ntri(T) + sizeof(uint32_t) * gramtc_ntri(T) + 64;
-  const size_t span = 3 * gramtc_tile_bytes(rows, T) + 8 * gramtc_sbo(rows);  // stage 1's lo + 8 groups
+  // an A operand spans 8 row groups from the last tile's start
+  const size_t span = (2 * (size_t)gramtc_parts(bf16) - 1) * gramtc_tile_bytes(rows, T, bf16) +
+                      8 * gramtc_sbo(rows, bf16);
   return end > span ? end : span;
 }
 __host__ __device__ inline int gramtc_npad(int T) { return (T + 7) & ~7; }
@@ -117,19 +159,21 @@ constexpr uint32_t kGramTcCols = 128;  // two accumulators of up to 64 columns
 // grid: nfull + (columns - nfull) * nsplit CTAs (columns cut into window
 // ranges as in gram_z_kernel); block: kGramTcThreads. T <= 64, T % 4 == 0,
 // px*py <= 128. ``gram`` points at the Gram block of patch col0 * ncz.
+template <bool BF16>
 __global__ void __launch_bounds__(kGramTcThreads)
     gram_tc_kernel(const __grid_constant__ CUtensorMap xmap, float* __restrict__ gram, Geom g, AxisTables tab,
                    long long col0, int ring, int nfull, int nsplit, int* status) {
   extern __shared__ __align__(1024) unsigned char smt[];
+  constexpr int NP = BF16 ? 3 : 2;  // split tiles per stage
   const int T = g.nt;
   const int rows = g.px * g.py;
-  const int kpad = gramtc_kpad(rows);
-  const uint32_t sbo = (uint32_t)gramtc_sbo(rows);  // bytes between 8-row groups
-  const size_t tile = gramtc_tile_bytes(rows, T);
+  const int kpad = gramtc_kpad(rows, BF16);
+  const uint32_t sbo = (uint32_t)gramtc_sbo(rows, BF16);  // bytes between 8-row groups
+  const size_t tile = gramtc_tile_bytes(rows, T, BF16);
   const size_t pf = gramz_plane_floats(rows, T);
   const int ntri = gramtc_ntri(T);
   const int TH = T + 1;  // H row stride (odd: conflict-free column writes)
-  float* planes = reinterpret_cast<float*>(smt + gramtc_off_plane(rows, T));  // two slots of pf floats
+  float* planes = reinterpret_cast<float*>(smt + gramtc_off_plane(rows, T, BF16));  // two slots of pf floats
   float* H = planes + 2 * pf;
   float* win = H + (size_t)T * TH;  // [ring][ntri]
   uint32_t* tri = reinterpret_cast<uint32_t*>(win + (size_t)ring * ntri);
@@ -151,12 +195,13 @@ __global__ void __launch_bounds__(kGramTcThreads)
   const int cx = tab.corners[0][ci], cy = tab.corners[1][cj];
   const uint32_t plane_bytes = (uint32_t)(rows * T * sizeof(float));
   const int Npad = gramtc_npad(T);
-  const uint32_t idesc = umma_idesc_tf32(64, Npad);
-  const int nv4 = (rows + 3) >> 2;
+  const uint32_t idesc = BF16 ? umma_idesc_bf16(64, Npad) : umma_idesc_tf32(64, Npad);
+  constexpr int KV = BF16 ? 8 : 4;  // voxels per 16-byte core-matrix row
+  const int nv4 = (rows + KV - 1) / KV;
 
   // zero both stages' operand tiles (rows >= T and voxels >= rows stay zero) and the windows;
   // the upper-triangle table
-  for (size_t e = tid; e < 4 * tile / 16; e += nth) reinterpret_cast<uint4*>(smt)[e] = make_uint4(0, 0, 0, 0);
+  for (size_t e = tid; e < 2 * NP * tile / 16; e += nth) reinterpret_cast<uint4*>(smt)[e] = make_uint4(0, 0, 0, 0);
   for (int e = tid; e < ring * ntri; e += nth) win[e] = 0.f;
   for (int r = warp; r < T; r += nth / 32) {
     const int base = r * T - r * (r - 1) / 2;  // index of (r, r)
@@ -264,11 +309,11 @@ __global__ void __launch_bounds__(kGramTcThreads)
       *abort_flag = 1;
     else if (tid == kIssuer)
       tma_pend[s] = false;
-    // split plane z into stage s's hi / lo K-major tiles; item (t, 4 voxels) ->
-    // one 16-byte core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16. Stage s
-    // was last read by plane z-2's MMAs, drained in step z-1.
+    // split plane z into stage s's K-major tiles; item (t, KV voxels) -> one
+    // 16-byte core-matrix row at (t/8)*SBO + v4*128 + (t%8)*16 in each tile.
+    // Stage s was last read by plane z-2's MMAs, drained in step z-1.
     const float* pl = planes + (size_t)s * pf;
-    unsigned char* hi = smt + (size_t)s * 2 * tile;
+    unsigned char* hi = smt + (size_t)s * NP * tile;
     unsigned char* lo = hi + tile;
     // item e = v4 * T + t, stepped by nth without a division per step
     const int dq = nth / T, dr = nth - (nth / T) * T;
@@ -278,17 +323,42 @@ __global__ void __launch_bounds__(kGramTcThreads)
         t -= T;
         ++v4;
       }
-      uint32_t hh[4], ll[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int v = 4 * v4 + i;
-        const float x = v < rows ? pl[v * T + t] : 0.f;
-        hh[i] = tf32_rna(x);
-        ll[i] = tf32_rna(x - __uint_as_float(hh[i]));
-      }
       const uint32_t off = (uint32_t)(t >> 3) * sbo + (uint32_t)v4 * 128 + (uint32_t)(t & 7) * 16;
-      *reinterpret_cast<uint4*>(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
-      *reinterpret_cast<uint4*>(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+      if constexpr (BF16) {
+        uint32_t b[3][4];  // three terms, 8 BF16 values each, packed in pairs
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          uint32_t lohalf[3], hihalf[3];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int v = KV * v4 + 2 * i + h;
+            const float x = v < rows ? pl[v * T + t] : 0.f;
+            const uint32_t b0 = bf16_bits(x);
+            const float r1 = x - bf16_value(b0);
+            const uint32_t b1 = bf16_bits(r1);
+            const uint32_t b2 = bf16_bits(r1 - bf16_value(b1));
+            (h ? hihalf : lohalf)[0] = b0;
+            (h ? hihalf : lohalf)[1] = b1;
+            (h ? hihalf : lohalf)[2] = b2;
+          }
+#pragma unroll
+          for (int q = 0; q < 3; ++q) b[q][i] = lohalf[q] | (hihalf[q] << 16);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+          *reinterpret_cast<uint4*>(hi + q * tile + off) = make_uint4(b[q][0], b[q][1], b[q][2], b[q][3]);
+      } else {
+        uint32_t hh[4], ll[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int v = 4 * v4 + i;
+          const float x = v < rows ? pl[v * T + t] : 0.f;
+          hh[i] = tf32_rna(x);
+          ll[i] = tf32_rna(x - __uint_as_float(hh[i]));
+        }
+        *reinterpret_cast<uint4*>(hi + off) = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+        *reinterpret_cast<uint4*>(lo + off) = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();  // tiles written, plane slot s free
@@ -300,19 +370,35 @@ __global__ void __launch_bounds__(kGramTcThreads)
         tma_par[s] = (uint32_t)(((it + 2) >> 1) & 1);
       }
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t hi_addr = smt_addr + (uint32_t)(s * 2 * tile), lo_addr = hi_addr + (uint32_t)tile;
+      const uint32_t hi_addr = smt_addr + (uint32_t)(s * NP * tile), lo_addr = hi_addr + (uint32_t)tile;
       const uint32_t acc_addr = tmem + (uint32_t)(s * 64);
-      // the descriptors' start-address field is address >> 4: one K step (8 tf32
-      // = two 128-byte core matrices) adds 16 to it
+      // the descriptors' start-address field is address >> 4: one K step (8 TF32
+      // or 16 BF16 = two 128-byte core matrices) adds 16 to it
       uint64_t dh = umma_desc_kmajor(hi_addr, 128, sbo), dl = umma_desc_kmajor(lo_addr, 128, sbo);
       uint32_t acc = 0;
-      for (int ks = 0; ks < kpad / 8; ++ks) {
-        umma_tf32(acc_addr, dh, dh, idesc, acc);
-        umma_tf32(acc_addr, dh, dl, idesc, 1);
-        umma_tf32(acc_addr, dl, dh, idesc, 1);
-        acc = 1;
-        dh += 16;
-        dl += 16;
+      if constexpr (BF16) {
+        uint64_t d2 = umma_desc_kmajor(lo_addr + (uint32_t)tile, 128, sbo);
+        for (int ks = 0; ks < kpad / 16; ++ks) {
+          umma_bf16(acc_addr, dh, dh, idesc, acc);
+          umma_bf16(acc_addr, dh, dl, idesc, 1);
+          umma_bf16(acc_addr, dl, dh, idesc, 1);
+          umma_bf16(acc_addr, dh, d2, idesc, 1);
+          umma_bf16(acc_addr, dl, dl, idesc, 1);
+          umma_bf16(acc_addr, d2, dh, idesc, 1);
+          acc = 1;
+          dh += 16;
+          dl += 16;
+          d2 += 16;
+        }
+      } else {
+        for (int ks = 0; ks < kpad / 8; ++ks) {
+          umma_tf32(acc_addr, dh, dh, idesc, acc);
+          umma_tf32(acc_addr, dh, dl, idesc, 1);
+          umma_tf32(acc_addr, dl, dh, idesc, 1);
+          acc = 1;
+          dh += 16;
+          dl += 16;
+        }
       }
       umma_commit(bar_mma(s));
       mma_pend[s] = true;

@@ -24,6 +24,7 @@
 #include "gram_z.cuh"
 #include "lrd_common.cuh"
 #include "recon.cuh"
+#include "recon_tc.cuh"
 #include "recon_warp.cuh"
 
 namespace {
@@ -71,9 +72,12 @@ struct lrd_plan {
   int tpt;                 // recon frames per thread
   int split;               // recon threads per voxel
   bool recon_warp = false; // reconstruction by recon_warp_kernel (2 x 2 x 2 voxels per warp)
+  bool recon_tc = false;   // reconstruction by recon_tc_kernel (tensor forms: 4 x 4 x 8 bricks on tcgen05)
+  size_t smem_recon_tc = 0;
   int gram_threads;
   bool use_gramz;          // column Gram kernel (TMA-staged z-planes) instead of per-patch
-  bool use_gramtc;         // the column Gram on tcgen05 (tensor form)
+  bool use_gramtc;         // the column Gram on tcgen05 (tensor forms)
+  bool gramtc_bf16 = false; // ... with BF16 3-term split operands instead of 3xTF32
   size_t smem_gramtc;
   int gramz_ring;          // window accumulator slots
   int gramz_ks = 1;        // voxel-row split per 4x4 Gram block (threads per block)
@@ -129,6 +133,10 @@ namespace {
 // against 0.96 ms unsplit and 1.27 ms with 4; T = 32, 64 and 96 are fastest
 // unsplit (0.58 / 1.44 / 1.21 ms, the split costing 30-60%).
 int gramz_split(int T) { return (T > 40 && T <= 56) ? 2 : 1; }
+
+void* gramtc_kernel_ptr(bool bf16) {
+  return bf16 ? (void*)lrd::gram_tc_kernel<true> : (void*)lrd::gram_tc_kernel<false>;
+}
 
 void* gramz_kernel_ptr(int ks) {
   switch (ks) {
@@ -286,6 +294,15 @@ void* recon_warp_ptr(int T, bool accurate) {
   return nullptr;
 }
 
+void* recon_tc_ptr(int T) {
+  switch (lrd::recon_tc_tn(T)) {
+    case 16: return (void*)lrd::recon_tc_kernel<16>;
+    case 32: return (void*)lrd::recon_tc_kernel<32>;
+    case 48: return (void*)lrd::recon_tc_kernel<48>;
+    default: return (void*)lrd::recon_tc_kernel<64>;
+  }
+}
+
 // The dynamic shared-memory limit is a property of the kernel, shared by
 // every plan in the process: only ever raise it (per device and kernel), so a
 // plan created later with a smaller need cannot shrink an earlier plan's.
@@ -396,8 +413,12 @@ int run_gram(const lrd_plan* P, char* ws, float* d_gram, cudaStream_t st, long l
       }
       const long long grid = nfull + (nc - nfull) * nsplit;
       if (P->use_gramtc) {
-        lrd::gram_tc_kernel<<<(unsigned)grid, lrd::kGramTcThreads, P->smem_gramtc, st>>>(
-            map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, (int)nfull, nsplit, status);
+        if (P->gramtc_bf16)
+          lrd::gram_tc_kernel<true><<<(unsigned)grid, lrd::kGramTcThreads, P->smem_gramtc, st>>>(
+              map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, (int)nfull, nsplit, status);
+        else
+          lrd::gram_tc_kernel<false><<<(unsigned)grid, lrd::kGramTcThreads, P->smem_gramtc, st>>>(
+              map, d_gram + c0 * P->g.ncz * TT, P->g, P->tab, c0, P->gramz_ring, (int)nfull, nsplit, status);
         rc = launch_check("gram_tc_kernel launch");
       } else {
         void* fn = gramz_kernel_ptr(P->gramz_ks);
@@ -502,17 +523,21 @@ int run_recon(const lrd_plan* P, char* ws, float* d_out, cudaStream_t st, long l
   const long long nbricks = (long long)P->g.nbx * P->g.nby * P->g.nbz;
   if (b_hi < 0) b_hi = nbricks;
   if (b_hi <= b_lo) return LRD_OK;
-  const unsigned threads =
-      P->recon_warp ? 32u * lrd::kReconWarps : (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
-  void* fn = P->recon_warp ? recon_warp_ptr(P->g.nt, acc) : recon_kernel_ptr(P->tpt, P->split, acc);
-  const size_t smem = P->recon_warp ? 0 : P->smem_recon;
+  const unsigned threads = P->recon_tc     ? (unsigned)lrd::kRtcThreads
+                           : P->recon_warp ? 32u * lrd::kReconWarps
+                                           : (unsigned)(P->g.bx * P->g.by * P->g.bz * P->split);
+  void* fn = P->recon_tc     ? recon_tc_ptr(P->g.nt)
+             : P->recon_warp ? recon_warp_ptr(P->g.nt, acc)
+                             : recon_kernel_ptr(P->tpt, P->split, acc);
+  const size_t smem = P->recon_tc ? P->smem_recon_tc : (P->recon_warp ? 0 : P->smem_recon);
   lrd::Geom g = P->g;
   lrd::AxisTables tab = P->tab;
   int brick0 = (int)b_lo;
   lrd::SlabIO sio{0, g.nx, 0, nullptr, g.nx, nullptr};
   if (io) sio = *io;
-  void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv, (void*)&rank, (void*)&wgt,
-                  (void*)&d_out, (void*)&g, (void*)&tab, (void*)&brick0, (void*)&sio};
+  int* status = reinterpret_cast<int*>(ws + P->off_status);
+  void* args[] = {(void*)&xc, (void*)&mean, (void*)&gv,  (void*)&rank,   (void*)&wgt,   (void*)&d_out,
+                  (void*)&g,  (void*)&tab,  (void*)&brick0, (void*)&sio, (void*)&status};
   cudaError_t e = cudaLaunchKernel(fn, dim3((unsigned)(b_hi - b_lo)), dim3(threads), args, smem, st);
   if (e != cudaSuccess) return cuda_fail(e, "recon_kernel launch");
   return LRD_OK;
@@ -540,7 +565,8 @@ int validate_problem(const lrd_problem* pr) {
   if (pr->nt < 2) return fail(LRD_ERR_INVALID, "need at least 2 frames, got %d", pr->nt);
   if (pr->nt > lrd::kMaxT) return fail(LRD_ERR_UNSUPPORTED, "nt=%d exceeds the compiled limit %d", pr->nt, lrd::kMaxT);
   if (pr->stride < 1) return fail(LRD_ERR_INVALID, "stride must be >= 1, got %d", pr->stride);
-  if (pr->form != LRD_FORM_PLAIN && pr->form != LRD_FORM_ACCURATE && pr->form != LRD_FORM_TENSOR)
+  if (pr->form != LRD_FORM_PLAIN && pr->form != LRD_FORM_ACCURATE && pr->form != LRD_FORM_TENSOR &&
+      pr->form != LRD_FORM_TENSOR_BF16)
     return fail(LRD_ERR_INVALID, "unknown form %d", pr->form);
   if (pr->batch < 0) return fail(LRD_ERR_INVALID, "batch must be >= 0, got %d", pr->batch);
   if (pr->recon_split != 0 && pr->recon_split != 1 && pr->recon_split != 2 && pr->recon_split != 4)
@@ -563,8 +589,21 @@ int validate_problem(const lrd_problem* pr) {
 // Measured on B200, reconstruction ms, 96x96x48x48 / 11^3 / stride 3:
 // brick kernel (3x3x3, 2 threads per voxel) 1.22 -> warp kernel (see DESIGN).
 int pick_layout(const lrd_problem* pr, const int dims[3], const int pat[3], const std::vector<int32_t> corners[3],
-                int& rsplit, int& rtpt, int best[3], bool* warp = nullptr) {
+                int& rsplit, int& rtpt, int best[3], bool* warp = nullptr, bool* tc = nullptr) {
   if (warp) *warp = false;
+  if (tc) *tc = false;
+  const char* tc_env = getenv("LRD_RECON_TC");  // "0": the tensor forms keep the warp kernel
+  if (tc && (pr->form == LRD_FORM_TENSOR || pr->form == LRD_FORM_TENSOR_BF16) && pr->recon_split == 0 &&
+      pr->brick_x == 0 && pr->brick_y == 0 && pr->brick_z == 0 && lrd::recon_tc_supported(pr->nt) &&
+      !(tc_env && tc_env[0] == '0')) {
+    *tc = true;
+    rsplit = 1;
+    rtpt = pr->nt;
+    best[0] = lrd::kRtcBX;
+    best[1] = lrd::kRtcBY;
+    best[2] = lrd::kRtcBZ;
+    return LRD_OK;
+  }
   if (warp && pr->recon_split == 0 && pr->brick_x == 0 && pr->brick_y == 0 && pr->brick_z == 0 &&
       lrd::recon_warp_supported(pr->nt)) {
     *warp = true;
@@ -635,8 +674,8 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   // brick shape
   int best[3] = {1, 1, 1};
   int rsplit = 1, rtpt = 4;
-  bool warp_recon = false;
-  if (int lrc = pick_layout(pr, dims, pat, corners, rsplit, rtpt, best, &warp_recon)) return lrc;
+  bool warp_recon = false, tc_recon = false;
+  if (int lrc = pick_layout(pr, dims, pat, corners, rsplit, rtpt, best, &warp_recon, &tc_recon)) return lrc;
   const int bsz[3] = {best[0], best[1], best[2]};
   for (int a = 0; a < 3; ++a) {
     const int nb = (dims[a] + bsz[a] - 1) / bsz[a];
@@ -702,6 +741,14 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   P->tpt = rtpt;
   P->split = rsplit;
   P->recon_warp = warp_recon;
+  P->recon_tc = tc_recon;
+  if (tc_recon) {
+    // the largest (y, z) patch box of a brick: one x corner's group of columns
+    int qy = 1, qz = 1;
+    for (size_t b = 0; b + 1 < brick[1].size(); b += 2) qy = std::max(qy, brick[1][b + 1] - brick[1][b] + 1);
+    for (size_t b = 0; b + 1 < brick[2].size(); b += 2) qz = std::max(qz, brick[2][b + 1] - brick[2][b] + 1);
+    P->smem_recon_tc = lrd::recon_tc_smem_bytes(T, qy * qz);
+  }
   const int nb4 = (T + 3) / 4;
   P->gram_threads = nb4 * (nb4 + 1) / 2;
   P->center_warps = 4;
@@ -717,14 +764,15 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     P->smem_gramz = lrd::gramz_smem_bytes(pr->px * pr->py, T, ring, P->gram_threads);
     P->use_gramz = (T % 4 == 0) && P->smem_gramz <= 200 * 1024 && tensor_map_encoder() != nullptr &&
                    pr->px <= 256 && pr->py <= 256;
-    P->smem_gramtc = lrd::gramtc_smem_bytes(pr->px * pr->py, T, ring);
-    P->use_gramtc = pr->form == LRD_FORM_TENSOR && T <= 64 && (T % 4 == 0) && pr->px * pr->py <= 128 &&
+    P->gramtc_bf16 = pr->form == LRD_FORM_TENSOR_BF16;
+    P->smem_gramtc = lrd::gramtc_smem_bytes(pr->px * pr->py, T, ring, P->gramtc_bf16);
+    P->use_gramtc = (pr->form == LRD_FORM_TENSOR || pr->form == LRD_FORM_TENSOR_BF16) && T <= 64 && (T % 4 == 0) && pr->px * pr->py <= 128 &&
                     P->smem_gramtc <= 200 * 1024 && tensor_map_encoder() != nullptr;
   }
   int rc = set_smem((const void*)lrd::center_kernel, P->smem_center);
   if (!rc) rc = set_smem((const void*)lrd::gram_kernel, P->smem_gram);
   if (!rc && P->use_gramz) rc = set_smem(gramz_kernel_ptr(P->gramz_ks), P->smem_gramz);
-  if (!rc && P->use_gramtc) rc = set_smem((const void*)lrd::gram_tc_kernel, P->smem_gramtc);
+  if (!rc && P->use_gramtc) rc = set_smem(gramtc_kernel_ptr(P->gramtc_bf16), P->smem_gramtc);
   P->smem_refine = lrd::eigh_refine_smem_bytes(T, pr->pz);
   if (!rc) rc = set_smem((const void*)lrd::eigh_refine_kernel, P->smem_refine);
   {
@@ -742,7 +790,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
         (void)cudaGetLastError();  // no cut columns; the launches report their own errors
     }
     if (!rc && P->use_gramtc) {
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lrd::gram_tc_kernel, lrd::kGramTcThreads,
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gramtc_kernel_ptr(P->gramtc_bf16), lrd::kGramTcThreads,
                                                         P->smem_gramtc) == cudaSuccess)
         P->gramtc_slots = per_sm * sms;
       else
@@ -750,15 +798,16 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
     }
   }
   if (!rc) rc = set_smem(eigh_kernel_for(T), P->smem_eigh);
-  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, false), P->smem_recon);
-  if (!rc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, true), P->smem_recon);
+  if (!rc && !P->recon_tc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, false), P->smem_recon);
+  if (!rc && !P->recon_tc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, true), P->smem_recon);
+  if (!rc && P->recon_tc) rc = set_smem(recon_tc_ptr(T), P->smem_recon_tc);
   if (rc) {
     cudaFree(P->d_tables);
     delete P;
     return rc;
   }
-  if (P->smem_gram > 227 * 1024 || P->smem_eigh > 227 * 1024 || P->smem_recon > 227 * 1024 ||
-      P->smem_refine > 227 * 1024) {
+  if (P->smem_gram > 227 * 1024 || P->smem_eigh > 227 * 1024 || (!P->recon_tc && P->smem_recon > 227 * 1024) ||
+      P->smem_refine > 227 * 1024 || P->smem_recon_tc > 227 * 1024) {
     cudaFree(P->d_tables);
     delete P;
     return fail(LRD_ERR_UNSUPPORTED, "patch plane or T too large for shared memory");

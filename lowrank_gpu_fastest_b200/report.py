@@ -180,7 +180,7 @@ def count_mismatches(ranks, ranks32, ranks64):
                 step0_vs_fp64=int((a != b).sum()))
 
 
-def rank_agreement(paths, forms=("plain", "accurate", "tensor")):
+def rank_agreement(paths, forms=("plain", "accurate", "tensor", "tensor_bf16")):
     """Rank agreement in the manner of the ladder's micro/rank_agreement.py:
     46-102 (which counts the MP-rank mismatches of FP32 routes against an FP64
     SVD): for every case file (an ``.npz`` with the input's generator, shape,
@@ -244,7 +244,7 @@ def main(argv=None):
     p.add_argument("--json", default=None)
     p = sub.add_parser("rank-agreement")
     p.add_argument("cases", nargs="+")
-    p.add_argument("--forms", default="plain,accurate,tensor")
+    p.add_argument("--forms", default="plain,accurate,tensor,tensor_bf16")
     a = ap.parse_args(argv)
     if a.cmd == "breakdown":
         r = phase_breakdown(a.shape, a.patch, a.stride, a.form, a.reps)

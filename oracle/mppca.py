@@ -157,6 +157,31 @@ def ranks_only(vol, patch=(11, 11, 11), step=3, corners=None):
     return ranks
 
 
+def patch_matrix(vol, corner, patch):
+    """The (N, T) Casorati matrix of the patch at ``corner`` (x-major voxels)."""
+    i, j, k = (int(c) for c in corner)
+    return vol[i:i + patch[0], j:j + patch[1], k:k + patch[2]].reshape(-1, vol.shape[-1])
+
+
+def mp_tie_scale(x):
+    """Distance of one patch's MP decision from a tie, in units of its largest
+    eigenvalue: min over indices i of |lhs_i - rhs_i| / (eigs_0 (t - i)(n - i))
+    with the float64 test of step0_numpy_loop.py:19-24 (eigs from a float64
+    SVD of the centred patch). An eigenvalue error below this fraction of the
+    largest eigenvalue cannot flip the count at index i through its own term.
+    """
+    x = np.asarray(x, dtype=np.float64)
+    n, t = x.shape
+    s = np.linalg.svd(x - x.mean(axis=1, keepdims=True), compute_uv=False)
+    t -= 1
+    eigs = s[:t] ** 2 / n
+    rcum = np.cumsum(eigs[::-1])[::-1]
+    i = np.arange(t)
+    lhs = (eigs - eigs[-1]) * (t - i) * (n - i)
+    rhs = 4 * rcum * np.sqrt(t * n)
+    return float(np.min(np.abs(lhs - rhs) / (eigs[0] * (t - i) * (n - i))))
+
+
 def gram_route_patch(x):
     """Step 4's U-free route on one patch, float64 (step4_gram_eigh.py:40-67).
 

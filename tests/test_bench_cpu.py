@@ -17,6 +17,9 @@ def test_phase_kernel_names():
     assert bench.phase_kernel("gram", 48, "plain") == "gram_z_kernel"
     assert bench.phase_kernel("gram", 48, "tensor") == "gram_tc_kernel"
     assert bench.phase_kernel("gram", 96, "tensor") == "gram_z_kernel"
+    assert bench.phase_kernel("gram", 48, "tensor_bf16") == "gram_tc_kernel"
+    assert bench.phase_kernel("recon", 48, "tensor") == "recon_tc_kernel"
+    assert bench.phase_kernel("recon", 96, "tensor") == "recon_warp_kernel"
     assert bench.phase_kernel("eigh_mp", 64, "plain") == "eigh_reg_kernel"
     assert bench.phase_kernel("eigh_mp", 96, "plain") == "eigh_cta_kernel"
     assert bench.phase_kernel("recon", 48, "plain") == "recon_warp_kernel"

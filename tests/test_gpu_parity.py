@@ -36,7 +36,7 @@ def test_small_plain_vs_step0(cuda_ok, name):
     assert rel_l2(out, g["out"]) <= PLAIN_TOL
 
 
-@pytest.mark.parametrize("form", ["accurate", "tensor"])
+@pytest.mark.parametrize("form", ["accurate", "tensor", "tensor_bf16"])
 @pytest.mark.parametrize("name", SMALL_CASES)
 def test_small_accurate_vs_fp64(cuda_ok, name, form):
     g = load_golden(name)
@@ -55,7 +55,7 @@ def test_large_ranks_and_sample(cuda_ok, name):
     np.testing.assert_array_equal(ranks, g["ranks"])
     idx = g["sample_idx"]
     assert rel_l2(out.reshape(-1)[idx], g["out_sample"]) <= PLAIN_TOL
-    for form in ("accurate", "tensor"):
+    for form in ("accurate", "tensor", "tensor_bf16"):
         outa, ra = run_dev(vol, tuple(g["patch"]), int(g["stride"]), form=form)
         np.testing.assert_array_equal(ra, g["ranks"])
         assert rel_l2(outa.reshape(-1)[idx], g["out64_sample"]) <= ACCURATE_TOL_LARGE
@@ -175,14 +175,16 @@ def test_error_is_raised_for_bad_shapes(cuda_ok):
         api.denoise(torch.zeros(4, 4, 4, 8, device="cuda"), (5, 5, 5), 2)
 
 
+@pytest.mark.parametrize("form", ["tensor", "tensor_bf16"])
 @pytest.mark.parametrize("name", ["lowrank_p5s2", "ref_small", "lowrank_t64", "aniso"])
-def test_tensor_core_gram_vs_fp64(cuda_ok, name):
-    """The tcgen05 3xTF32 Gram (tensor form) against float64 Grams of the
-    same centred patches: within 4e-6 of the largest entry (FP32 FFMA: ~1e-6)."""
+def test_tensor_core_gram_vs_fp64(cuda_ok, name, form):
+    """The tcgen05 Grams (3xTF32 and 3-term BF16 split products) against
+    float64 Grams of the same centred patches: within 4e-6 of the largest
+    entry (FP32 FFMA: ~1e-6)."""
     g = load_golden(name)
     vol = golden_input(g)
     shape, patch, stride = vol.shape, tuple(int(v) for v in g["patch"]), int(g["stride"])
-    plan = api.get_plan(shape, patch, stride, form="tensor")
+    plan = api.get_plan(shape, patch, stride, form=form)
     T, P = shape[3], plan.n_patches
     d = torch.from_numpy(vol).cuda()
     ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device="cuda")
@@ -225,7 +227,7 @@ def test_bounded_wait_gives_up_and_reports(cuda_ok):
 def test_status_word_clear_after_runs(cuda_ok):
     g = load_golden("ref_small")
     vol = torch.from_numpy(golden_input(g)).cuda()
-    for form in ("plain", "tensor"):
+    for form in ("plain", "tensor", "tensor_bf16"):
         plan = api.get_plan(tuple(vol.shape), (11, 11, 11), 3, form=form)
         ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device="cuda")
         out = torch.empty_like(vol)

@@ -18,7 +18,7 @@ def test_rank_agreement_all_cases_and_forms(cuda_ok):
     paths = [os.path.join(GOLDEN, f"{n}.npz") for n in SMALL_CASES + LARGE_CASES]
     rows = report.rank_agreement(paths)
     print("\n" + report.rank_table(rows))
-    assert len(rows) == 3 * len(paths)
+    assert len(rows) == 4 * len(paths)
     for r in rows:
         assert r["vs_step0"] == 0, r
         assert r["vs_fp64"] == r["step0_vs_fp64"], r

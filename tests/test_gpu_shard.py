@@ -48,7 +48,7 @@ def unsharded(vol, patch, stride, form):
     return out.cpu().numpy(), ranks.cpu().numpy()
 
 
-@pytest.mark.parametrize("form", ["plain", "accurate", "tensor"])
+@pytest.mark.parametrize("form", ["plain", "accurate", "tensor", "tensor_bf16"])
 @pytest.mark.parametrize("n", [2, 3])
 def test_slabs_equal_unsharded(cuda_ok, form, n):
     vol = make_phantom_lowrank((40, 20, 18, 32), seed=5)[0]

@@ -27,8 +27,8 @@ PLAIN_TOL = 2e-7
 # relative L2 between the static path and lrd_denoise, per form: both follow the
 # same arithmetic except the Gram (per-patch kernel here, column kernel in the
 # plan path; for the tensor form the plan path's Gram is tcgen05 3xTF32)
-FORM_TOL = {0: PLAIN_TOL, 1: 1e-7, 2: 1e-7}
-FORM_NAME = {0: "plain", 1: "accurate", 2: "tensor"}
+FORM_TOL = {0: PLAIN_TOL, 1: 1e-7, 2: 1e-7, 3: 1e-7}
+FORM_NAME = {0: "plain", 1: "accurate", 2: "tensor", 3: "tensor_bf16"}
 
 
 def _problem(shape, patch, stride, form=0):
@@ -48,7 +48,7 @@ def _static_call(vol_dev, patch, stride, form=0):
     return out.cpu().numpy(), ranks.cpu().numpy()
 
 
-@pytest.mark.parametrize("form", [0, 1, 2])
+@pytest.mark.parametrize("form", [0, 1, 2, 3])
 def test_static_entry_matches_plan_entry_twice(cuda_ok, form):
     g = load_golden("config1_lowrank")
     vol = torch.from_numpy(golden_input(g)).cuda()
