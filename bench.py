@@ -686,8 +686,9 @@ def run_ours(args, wl):
 
     extra = {}
     if world == 1 and not args.single_form:
-        # the other forms beside the timed one: accurate meets the float64 bar
-        for f in ("plain", "accurate"):
+        # the other forms beside the timed one: accurate and the tensor-core forms
+        # meet the float64 bar
+        for f in ("plain", "accurate", "tensor", "tensor_bf16"):
             if f != args.form:
                 r = time_form(torch, dist, args, wl, f, vol, rank, world, local, golden=golden)
                 extra[f] = r

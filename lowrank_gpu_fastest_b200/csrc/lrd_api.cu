@@ -593,9 +593,23 @@ int pick_layout(const lrd_problem* pr, const int dims[3], const int pat[3], cons
   if (warp) *warp = false;
   if (tc) *tc = false;
   const char* tc_env = getenv("LRD_RECON_TC");  // "0": the tensor forms keep the warp kernel
+  // the largest patch box a 4 x 4 x 8 brick touches (per axis: corners whose
+  // patch meets the brick's range), which the tensor-core kernel keeps in
+  // shared memory
+  auto box_side = [&](int a, int bs) {
+    long long most = 0;
+    for (int lo = 0; lo < dims[a]; lo += bs) {
+      const int hi = std::min(dims[a], lo + bs) - 1;
+      long long cnt = 0;
+      for (int c : corners[a]) cnt += (c <= hi && c + pat[a] - 1 >= lo);
+      most = std::max(most, cnt);
+    }
+    return most;
+  };
   if (tc && (pr->form == LRD_FORM_TENSOR || pr->form == LRD_FORM_TENSOR_BF16) && pr->recon_split == 0 &&
       pr->brick_x == 0 && pr->brick_y == 0 && pr->brick_z == 0 && lrd::recon_tc_supported(pr->nt) &&
-      !(tc_env && tc_env[0] == '0')) {
+      !(tc_env && tc_env[0] == '0') &&
+      box_side(0, lrd::kRtcBX) * box_side(1, lrd::kRtcBY) * box_side(2, lrd::kRtcBZ) <= lrd::kRtcMaxBoxPatches) {
     *tc = true;
     rsplit = 1;
     rtpt = pr->nt;
@@ -743,11 +757,12 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   P->recon_warp = warp_recon;
   P->recon_tc = tc_recon;
   if (tc_recon) {
-    // the largest (y, z) patch box of a brick: one x corner's group of columns
-    int qy = 1, qz = 1;
+    // the largest patch box of a brick (its touching patches, one group per x corner)
+    int qx = 1, qy = 1, qz = 1;
+    for (size_t b = 0; b + 1 < brick[0].size(); b += 2) qx = std::max(qx, brick[0][b + 1] - brick[0][b] + 1);
     for (size_t b = 0; b + 1 < brick[1].size(); b += 2) qy = std::max(qy, brick[1][b + 1] - brick[1][b] + 1);
     for (size_t b = 0; b + 1 < brick[2].size(); b += 2) qz = std::max(qz, brick[2][b + 1] - brick[2][b] + 1);
-    P->smem_recon_tc = lrd::recon_tc_smem_bytes(T, qy * qz);
+    P->smem_recon_tc = lrd::recon_tc_smem_bytes(T, qx * qy * qz, qx);
   }
   const int nb4 = (T + 3) / 4;
   P->gram_threads = nb4 * (nb4 + 1) / 2;

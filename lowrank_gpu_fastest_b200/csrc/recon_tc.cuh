@@ -25,31 +25,37 @@
 //    2^-11 smaller) in two accumulators, added in FP32 on the CUDA cores;
 //  * GEMM 2 gives each K step (8 columns) its own accumulator (three MMAs,
 //    the first one overwriting), and the CUDA cores add the K steps' sums
-//    into a per-voxel float64 accumulator in registers.
+//    into a per-voxel FP32 accumulator in registers (round to nearest).
 // The weight sums are float64 (exact: a few hundred float32 values 1/(2+p)).
 //
 // Columns are taken in groups of one x corner index (every touching patch
 // (i, j, k) of the brick with the same i, j-major then k, then the patch's
 // eigenvectors in order), each group cut into chunks of kRtcChunk columns
 // (the last one zero-padded). A chunk never mixes two x corners, so a voxel's
-// float64 sum is the same sequence of additions whichever x-slab computes
-// which of its patches: a slab that hands its partial sums on (SlabIO halo)
-// and the next slab that continues from them give bit-identical results to
-// one unsharded call.
+// sum is the same sequence of additions whichever x-slab computes which of
+// its patches: a slab that hands its partial sums on (SlabIO halo, an exact
+// float64 copy) and the next slab that continues from them give
+// bit-identical results to one unsharded call.
 //
+// Per brick, once: the X tiles split into shared memory; the touching
+// patches' indices, ranks, weights and cover masks into a shared table, and
+// each x-corner group's rank prefix sums (so a chunk's column table is a
+// binary search in shared memory); each voxel's weight sum.
 // Per chunk (128 threads, thread v = voxel v = TMEM lane v):
-//   1. column table (eigenvector row, cover mask, weight) and the chunk's
-//      eigenvector rows, split hi / lo into shared memory twice: as GEMM 1's
-//      B (rows = columns, K = frames) and transposed as GEMM 2's B (rows =
-//      frames, K = columns), both K-major (an MN-major B operand of kind::tf32
-//      read back zeros here);
+//   1. the chunk's eigenvector rows (fetched into registers during the
+//      previous chunk), split hi / lo into shared memory twice: as GEMM 1's
+//      B (rows = columns, K = frames) and, through a raw copy, transposed as
+//      GEMM 2's B (rows = frames, K = columns), both K-major (an MN-major B
+//      operand of kind::tf32 read back zeros here);
 //   2. GEMM 1 into TMEM columns [0, C) (hi.hi) and [C, 2C) (cross terms);
+//      meanwhile the next chunk's column table is built and its rows are
+//      fetched;
 //   3. each thread reads its row of Y, scales it by S, splits it and writes
 //      Y~ hi / lo over the same columns (GEMM 2's A operand, in TMEM);
 //   4. GEMM 2, K step s into columns [2C + s Tn, 2C + (s + 1) Tn);
-//   5. each thread adds the K steps' sums into its float64 accumulator.
-// The X tiles are split into shared memory once per brick; two CTAs share an
-// SM (T <= 48: 256 TMEM columns and about 74 KB of shared memory each).
+//   5. each thread adds the K steps' sums into its accumulator.
+// Two CTAs share an SM (T <= 48: 256 TMEM columns and about 85 KB of shared
+// memory each at the headline).
 //
 // Waits on MMA completion are bounded by %globaltimer deadlines as in the
 // tensor-core Gram: a wait that gives up records kStatusMmaTimeout, the CTA
@@ -78,14 +84,20 @@ __host__ __device__ constexpr uint32_t recon_tc_tmem_cols(int Tn) {
 }
 
 // Shared-memory layout (bytes): X hi, X lo (128 x Tk each, K-major core
-// matrices), V hi, V lo (C rows x Tn), V^T hi, V^T lo (Tn rows x C), the
-// chunk's column table (C x {row offset (8), mask (4), weight (4)}),
-// mbarrier, TMEM address, abort flag, the group's rank prefix sums (qcap + 1
-// ints).
+// matrices), V hi, V lo (C rows x Tn), V^T hi, V^T lo (Tn rows x C), raw
+// rows for the transpose (C x (Tn + 4) floats), two column tables (C x {row
+// offset (8), mask (4), weight (4)} each), mbarrier, TMEM address, abort
+// flag, the brick's touching patches (npb of them: index (8), cover mask,
+// weight, rank (4 each)) and each x-corner group's rank prefix sums (npb +
+// groups ints).
 __host__ __device__ inline size_t recon_tc_xbytes(int T) { return (size_t)128 * recon_tc_tk(T) * 4; }
 __host__ __device__ inline size_t recon_tc_vbytes(int T) { return (size_t)kRtcChunk * recon_tc_tn(T) * 4; }
-__host__ __device__ inline size_t recon_tc_smem_bytes(int T, int qcap) {
-  return 2 * recon_tc_xbytes(T) + 4 * recon_tc_vbytes(T) + (size_t)kRtcChunk * 16 + 16 + (size_t)4 * (qcap + 1);
+// a brick whose patch box holds more patches than this (small strides with
+// large patches) takes the warp kernel instead
+constexpr int kRtcMaxBoxPatches = 1024;
+__host__ __device__ inline size_t recon_tc_smem_bytes(int T, int npb, int ngroups) {
+  return 2 * recon_tc_xbytes(T) + 4 * recon_tc_vbytes(T) + (size_t)kRtcChunk * (recon_tc_tn(T) + 4) * 4 +
+         (size_t)kRtcChunk * 32 + 24 + 20 * (size_t)npb + 4 * ((size_t)npb + ngroups);
 }
 
 // Instruction descriptor: kind::tf32, D = F32, M = 128, A and B K-major.
@@ -181,7 +193,7 @@ __device__ __noinline__ void rtc_issue_gemm2(uint32_t tmem, uint32_t thi_a, uint
 
 // One CTA: brick brick0 + bid of the plan's 4 x 4 x 8 brick grid (x-major).
 // Thread v owns voxel (x0 + v / 32, y0 + (v / 8) % 4, z0 + v % 8), MMA row v.
-// TN = recon_tc_tn(T): the per-voxel float64 accumulator lives in registers.
+// TN = recon_tc_tn(T): the per-voxel accumulator lives in registers.
 template <int TN>
 __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, const float* __restrict__ mean,
                                               const float* __restrict__ vecs, const int32_t* __restrict__ ranks,
@@ -192,21 +204,26 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
   constexpr int C = kRtcChunk;
   constexpr int KS2 = C / 8;  // GEMM 2 K steps per chunk
   static_assert(KS2 == 4, "the K-step sums are added as (s0 + s1) + (s2 + s3)");
+  constexpr int NG = TN / 4;                       // frame groups of an eigenvector row
+  constexpr int ITEMS = C * NG / kRtcThreads;      // row float4s per thread per chunk
+  constexpr int TITEMS = TN * (C / 4) / kRtcThreads;  // transposed units per thread per chunk
+  static_assert(ITEMS * kRtcThreads == C * NG && TITEMS * kRtcThreads == TN * (C / 4), "whole items per thread");
+  constexpr int RS = TN + 4;                       // raw row stride (floats)
   constexpr uint32_t kCols = recon_tc_tmem_cols(TN);
   extern __shared__ __align__(1024) unsigned char smr[];
   const int T = g.nt;
   const int Tk = recon_tc_tk(T);
   const size_t xb = recon_tc_xbytes(T), vb = recon_tc_vbytes(T);
   unsigned char* Xhi = smr;
-  unsigned char* Vhi = smr + 2 * xb;
-  unsigned char* Thi = Vhi + 2 * vb;                               // V^T hi, lo
-  long long* c_row = reinterpret_cast<long long*>(Thi + 2 * vb);  // eigenvector row offset, -1 = padding
-  uint32_t* c_mask = reinterpret_cast<uint32_t*>(c_row + C);      // cover bits: x (4) | y (4) << 4 | z (8) << 8
-  float* c_w = reinterpret_cast<float*>(c_mask + C);              // patch weight
-  uint64_t* bar = reinterpret_cast<uint64_t*>(c_w + C);
+  unsigned char* Vhi = smr + 2 * xb;                               // V hi, lo (rows = columns)
+  unsigned char* Thi = Vhi + 2 * vb;                               // V^T hi, lo (rows = frames)
+  float* raw = reinterpret_cast<float*>(Thi + 2 * vb);             // C x RS raw rows (transpose)
+  long long* c_row = reinterpret_cast<long long*>(raw + C * RS);   // [2][C] eigenvector row offset, -1 = padding
+  uint32_t* c_mask = reinterpret_cast<uint32_t*>(c_row + 2 * C);   // [2][C] cover bits: x | y << 4 | z << 8
+  float* c_w = reinterpret_cast<float*>(c_mask + 2 * C);           // [2][C] patch weight
+  uint64_t* bar = reinterpret_cast<uint64_t*>(c_w + 2 * C);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
-  int* qoff = abort_flag + 1;  // group rank prefix sums, nq + 1
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   int brick = brick0 + bid;
@@ -224,7 +241,13 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
   const int ilo = tab.brick[0][2 * bxi], ihi = tab.brick[0][2 * bxi + 1];
   const int jlo = tab.brick[1][2 * byi], jhi = tab.brick[1][2 * byi + 1];
   const int klo = tab.brick[2][2 * bzi], khi = tab.brick[2][2 * bzi + 1];
-  const int nk = khi - klo + 1, nq = (jhi - jlo + 1) * nk;
+  const int ni = max(ihi - ilo + 1, 0), nk = max(khi - klo + 1, 0), nq = max(jhi - jlo + 1, 0) * nk;
+  const int npb = ni * nq;  // the brick's touching patches: x-corner group a, then (j, k) j-major
+  long long* pb_pid = reinterpret_cast<long long*>(tmem_slot + 4);
+  uint32_t* pb_mask = reinterpret_cast<uint32_t*>(pb_pid + npb);
+  float* pb_w = reinterpret_cast<float*>(pb_mask + npb);
+  int* pb_rank = reinterpret_cast<int*>(pb_w + npb);
+  int* goff = pb_rank + npb;  // group a's rank prefix sums at a (nq + 1)
 
   const uint32_t bar_addr = (uint32_t)__cvta_generic_to_shared(bar);
   if (tid == 0) {
@@ -242,37 +265,75 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
 
   // X hi / lo: row tid, frame group fg -> (tid / 8) * SBO + fg * 128 + (tid % 8) * 16
   const uint32_t sbox = (uint32_t)Tk * 32, sbov = (uint32_t)TN * 32, sbot = (uint32_t)C * 32;
-  for (int fg = 0; fg < Tk / 4; ++fg) {
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid && 4 * fg < T) v = __ldg(reinterpret_cast<const float4*>(xc + row * T) + fg);
-    uint4 h, l;
-    rtc_split4(v, h, l);
-    const uint32_t off = (uint32_t)(tid >> 3) * sbox + (uint32_t)fg * 128 + (uint32_t)(tid & 7) * 16;
-    *reinterpret_cast<uint4*>(Xhi + off) = h;
-    *reinterpret_cast<uint4*>(Xhi + xb + off) = l;
-  }
-  // float64 sums: weights over the covering patches (exact) and the
-  // reconstruction, continuing a lower slab's partial sums
-  double acc[TN];
+  {
+    float4 xv[TN / 4];
 #pragma unroll
-  for (int f = 0; f < TN; ++f) acc[f] = 0.0;
+    for (int fg = 0; fg < TN / 4; ++fg)
+      xv[fg] = (valid && 4 * fg < T) ? __ldg(reinterpret_cast<const float4*>(xc + row * T) + fg)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int fg = 0; fg < TN / 4; ++fg) {
+      if (4 * fg >= Tk) break;
+      uint4 h, l;
+      rtc_split4(xv[fg], h, l);
+      const uint32_t off = (uint32_t)(tid >> 3) * sbox + (uint32_t)fg * 128 + (uint32_t)(tid & 7) * 16;
+      *reinterpret_cast<uint4*>(Xhi + off) = h;
+      *reinterpret_cast<uint4*>(Xhi + xb + off) = l;
+    }
+  }
+  // the brick's patches: index, rank, weight, cover mask
+  for (int idx = tid; idx < npb; idx += kRtcThreads) {
+    const int a = idx / nq, q = idx - a * nq;
+    const int cj = jlo + q / nk, ck = klo + q % nk;
+    const long long pid = ((long long)(ilo + a) * g.ncy + cj) * g.ncz + ck;
+    pb_pid[idx] = pid;
+    pb_rank[idx] = __ldg(ranks + pid);
+    pb_w[idx] = __ldg(wgt + pid);
+    pb_mask[idx] = rtc_axis_mask(tab.corners[0][ilo + a], g.px, x0, kRtcBX) |
+                   (rtc_axis_mask(tab.corners[1][cj], g.py, y0, kRtcBY) << 4) |
+                   (rtc_axis_mask(tab.corners[2][ck], g.pz, z0, kRtcBZ) << 8);
+  }
+  // the reconstruction sums (FP32, round to nearest) and the weight sum
+  // (float64: exact), continuing a lower slab's partial sums
+  float acc[TN];
+#pragma unroll
+  for (int f = 0; f < TN; ++f) acc[f] = 0.f;
   double wsum = 0.0;
   if (valid && x < io.hin && io.halo_in != nullptr) {
     const double* hp = io.halo_in + row * (T + 1);
 #pragma unroll
     for (int f = 0; f < TN; ++f)
-      if (f < T) acc[f] = hp[f];
+      if (f < T) acc[f] = (float)hp[f];
     wsum = hp[T];
   }
-  if (valid) {
+  __syncthreads();  // patch table written
+  if (valid) {  // weights of the covering patches, all inside the brick's box
     const int cxlo = tab.cover[0][2 * x], cxhi = tab.cover[0][2 * x + 1];
     const int cylo = tab.cover[1][2 * y], cyhi = tab.cover[1][2 * y + 1];
     const int czlo = tab.cover[2][2 * z], czhi = tab.cover[2][2 * z + 1];
     for (int i = cxlo; i <= cxhi; ++i)
       for (int j = cylo; j <= cyhi; ++j) {
-        const long long p0 = ((long long)i * g.ncy + j) * g.ncz;
-        for (int k = czlo; k <= czhi; ++k) wsum += (double)__ldg(wgt + p0 + k);
+        const float* wr = pb_w + (i - ilo) * nq + (j - jlo) * nk - klo;
+        for (int k = czlo; k <= czhi; ++k) wsum += (double)wr[k];
       }
+  }
+  if (warp == 0) {  // each x-corner group's rank prefix sums
+    for (int a = 0; a < ni; ++a) {
+      int* qo = goff + a * (nq + 1);
+      int carry = 0;
+      for (int q0 = 0; q0 < nq; q0 += 32) {
+        const int q = q0 + lane;
+        int sc = q < nq ? pb_rank[a * nq + q] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, sc, o);
+          if (lane >= o) sc += t;
+        }
+        if (q < nq) qo[q + 1] = carry + sc;
+        carry += __shfl_sync(0xffffffffu, sc, 31);
+      }
+      if (lane == 0) qo[0] = 0;
+    }
   }
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -287,16 +348,17 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
   uint32_t phase = 0;  // parity of the barrier's next phase
   bool pend = false;   // thread 0: a commit in flight
   uint32_t pend_phase = 0;
-  constexpr int NG = TN / 4;  // frame groups of a V row
 
-  // Issues the MMAs of one step (thread 0), commits them to the barrier and
-  // waits (every thread, bounded); a wait that gives up sets the abort flag.
-  auto commit_wait = [&]() {
+  // Commits the MMAs issued so far (thread 0) and waits for them (every
+  // thread, bounded); a wait that gives up sets the abort flag.
+  auto commit = [&]() {
     if (tid == 0) {
       umma_commit(bar_addr);
       pend = true;
       pend_phase = phase;
     }
+  };
+  auto wait = [&]() {
     if (!mbar_wait_bounded(bar_addr, phase, status, kStatusMmaTimeout))
       *abort_flag = 1;
     else if (tid == 0)
@@ -304,135 +366,149 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   };
-
-  for (int ci = ilo; ci <= ihi; ++ci) {
-    // the group's rank prefix sums (j-major, k inner)
-    __syncthreads();  // the previous group's table is no longer read
-    if (warp == 0) {
-      int carry = 0;
-      for (int q0 = 0; q0 < nq; q0 += 32) {
-        const int q = q0 + lane;
-        int r = 0;
-        if (q < nq) r = __ldg(ranks + ((long long)ci * g.ncy + jlo + q / nk) * g.ncz + klo + q % nk);
-        int sc = r;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, sc, o);
-          if (lane >= o) sc += t;
+  // chunk iterator: x-corner group a, first column c0 (a == ni: done)
+  auto ncol_of = [&](int a) { return goff[a * (nq + 1) + nq]; };
+  auto advance = [&](int& a, int& c0) {
+    c0 += C;
+    while (a < ni && c0 >= ncol_of(a)) {
+      ++a;
+      c0 = 0;
+    }
+  };
+  // column table of chunk (a, c0) into table buffer tb (threads < C)
+  auto table = [&](int a, int c0, int tb) {
+    if (tid < C) {
+      const int* qo = goff + a * (nq + 1);
+      const int ncol = qo[nq];
+      const int col = c0 + tid;
+      long long ro = -1;
+      uint32_t m = 0;
+      float w = 0.f;
+      if (col < ncol) {
+        int lo = 0, hi = nq - 1;  // largest q with qo[q] <= col: the patch holding the column
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (qo[mid] <= col)
+            lo = mid;
+          else
+            hi = mid - 1;
         }
-        if (q < nq) qoff[q + 1] = carry + sc;
-        carry += __shfl_sync(0xffffffffu, sc, 31);
+        const int idx = a * nq + lo;
+        ro = pb_pid[idx] * T * T + (long long)(col - qo[lo]) * T;
+        m = pb_mask[idx];
+        w = pb_w[idx];
       }
-      if (lane == 0) qoff[0] = 0;
+      c_row[tb * C + tid] = ro;
+      c_mask[tb * C + tid] = m;
+      c_w[tb * C + tid] = w;
+    }
+  };
+  // the chunk's eigenvector rows into registers: item e = tid + 128 i ->
+  // column e % C, frame group e / C
+  float4 vr[ITEMS];
+  auto fetch = [&](int tb) {
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const int e = tid + kRtcThreads * i, pos = e % C, fg = e / C;
+      const long long ro = c_row[tb * C + pos];
+      vr[i] = (ro >= 0 && 4 * fg < T) ? __ldg(reinterpret_cast<const float4*>(vecs + ro) + fg)
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+
+  int ca = 0, cc0 = 0;  // current chunk
+  while (ca < ni && ncol_of(ca) == 0) ++ca;
+  int tb = 0;
+  if (ca < ni) {
+    table(ca, cc0, 0);
+    __syncthreads();
+    fetch(0);
+  }
+  while (ca < ni) {
+    // 1. V (rows = columns) hi / lo from the fetched rows, and a raw copy
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+      const int e = tid + kRtcThreads * i, pos = e % C, fg = e / C;
+      uint4 h, l;
+      rtc_split4(vr[i], h, l);
+      const uint32_t off = (uint32_t)(pos >> 3) * sbov + (uint32_t)fg * 128 + (uint32_t)(pos & 7) * 16;
+      *reinterpret_cast<uint4*>(Vhi + off) = h;
+      *reinterpret_cast<uint4*>(Vhi + vb + off) = l;
+      *reinterpret_cast<float4*>(raw + pos * RS + 4 * fg) = vr[i];
     }
     __syncthreads();
-    if (*abort_flag) break;  // uniform: set before the barrier above
-    const int ncol = qoff[nq];
-    const uint32_t xmask = rtc_axis_mask(tab.corners[0][ci], g.px, x0, kRtcBX);
-    for (int c0 = 0; c0 < ncol; c0 += C) {
-      // 1. the chunk's column table, then its eigenvector rows split into V hi / lo
-      if (tid < C) {
-        const int c = c0 + tid;
-        long long ro = -1;
-        uint32_t m = 0;
-        float w = 0.f;
-        if (c < ncol) {
-          int lo = 0, hi = nq - 1;  // largest q with qoff[q] <= c: the patch holding column c
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (qoff[mid] <= c)
-              lo = mid;
-            else
-              hi = mid - 1;
-          }
-          const int cj = jlo + lo / nk, ck = klo + lo % nk;
-          const long long pid = ((long long)ci * g.ncy + cj) * g.ncz + ck;
-          ro = pid * T * T + (long long)(c - qoff[lo]) * T;
-          m = xmask | (rtc_axis_mask(tab.corners[1][cj], g.py, y0, kRtcBY) << 4) |
-              (rtc_axis_mask(tab.corners[2][ck], g.pz, z0, kRtcBZ) << 8);
-          w = __ldg(wgt + pid);
-        }
-        c_row[tid] = ro;
-        c_mask[tid] = m;
-        c_w[tid] = w;
-      }
-      __syncthreads();
-      // column pos, frame group fg -> (pos / 8) * SBO + fg * 128 + (pos % 8) * 16
-      for (int e = tid; e < C * NG; e += kRtcThreads) {
-        const int pos = e % C, fg = e / C;
-        const long long ro = c_row[pos];
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ro >= 0 && 4 * fg < T) v = __ldg(reinterpret_cast<const float4*>(vecs + ro) + fg);
-        uint4 h, l;
-        rtc_split4(v, h, l);
-        const uint32_t off = (uint32_t)(pos >> 3) * sbov + (uint32_t)fg * 128 + (uint32_t)(pos & 7) * 16;
-        *reinterpret_cast<uint4*>(Vhi + off) = h;
-        *reinterpret_cast<uint4*>(Vhi + vb + off) = l;
-      }
-      // V^T: frame f, column group cg -> (f / 8) * SBO + cg * 128 + (f % 8) * 16
-      for (int e = tid; e < TN * (C / 4); e += kRtcThreads) {
-        const int f = e % TN, cg = e / TN;
-        float vv[4];
+    // V^T (rows = frames): frame f, column group cg -> (f / 8) * SBO + cg * 128 + (f % 8) * 16
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const long long ro = c_row[4 * cg + i];
-          vv[i] = (ro >= 0 && f < T) ? __ldg(vecs + ro + f) : 0.f;
-        }
-        uint4 h, l;
-        rtc_split4(make_float4(vv[0], vv[1], vv[2], vv[3]), h, l);
-        const uint32_t off = (uint32_t)(f >> 3) * sbot + (uint32_t)cg * 128 + (uint32_t)(f & 7) * 16;
-        *reinterpret_cast<uint4*>(Thi + off) = h;
-        *reinterpret_cast<uint4*>(Thi + vb + off) = l;
-      }
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
-      // 2. GEMM 1: hi.hi into [0, C), hi.lo + lo.hi into [C, 2C)
-      if (tid == 0) rtc_issue_gemm1(tmem, xhi_a, (uint32_t)xb, sbox, vhi_a, (uint32_t)vb, sbov, Tk, idesc1);
-      commit_wait();
-      // 3. Y~ = S o Y, split: hi over [0, C), lo over [C, 2C)
-#pragma unroll 1
-      for (int j = 0; j < C; j += 16) {
-        uint32_t dh[16], dx[16];
-        tmem_ld16_nowait(tl + (uint32_t)j, dh);
-        tmem_ld16_nowait(tl + (uint32_t)(C + j), dx);
-        tmem_ld_wait();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const float sc = ((c_mask[j + i] & vbits) == vbits) ? c_w[j + i] : 0.f;
-          const float yv = __fmul_rn(__fadd_rn(__uint_as_float(dh[i]), __uint_as_float(dx[i])), sc);
-          dh[i] = tf32_rna(yv);
-          dx[i] = tf32_rna(__fsub_rn(yv, __uint_as_float(dh[i])));
-        }
-        tmem_st16(tl + (uint32_t)j, dh);
-        tmem_st16(tl + (uint32_t)(C + j), dx);
-      }
-      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();
-      if (*abort_flag) break;  // uniform
-      // 4. GEMM 2: K step s -> its own accumulator [2C + s TN, 2C + (s + 1) TN)
-      if (tid == 0) rtc_issue_gemm2(tmem, thi_a, (uint32_t)vb, sbot, TN, idesc2);
-      commit_wait();
-      // 5. the K steps' sums into the float64 accumulator ((s0 + s1) + (s2 + s3) in FP32)
-#pragma unroll
-      for (int f0 = 0; f0 < TN; f0 += 8) {
-        uint32_t r[KS2][8];
-#pragma unroll
-        for (int ks = 0; ks < KS2; ++ks) tmem_ld8_nowait(tl + (uint32_t)(2 * C + ks * TN + f0), r[ks]);
-        tmem_ld_wait();
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const float a01 = __fadd_rn(__uint_as_float(r[0][i]), __uint_as_float(r[1][i]));
-          const float a23 = __fadd_rn(__uint_as_float(r[2][i]), __uint_as_float(r[3][i]));
-          acc[f0 + i] += (double)__fadd_rn(a01, a23);
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      __syncthreads();  // V, the column table and the TMEM columns are free for the next chunk
-      if (*abort_flag) break;
+    for (int i = 0; i < TITEMS; ++i) {
+      const int e = tid + kRtcThreads * i, f = e % TN, cg = e / TN;
+      uint4 h, l;
+      rtc_split4(make_float4(raw[(4 * cg) * RS + f], raw[(4 * cg + 1) * RS + f], raw[(4 * cg + 2) * RS + f],
+                             raw[(4 * cg + 3) * RS + f]),
+                 h, l);
+      const uint32_t off = (uint32_t)(f >> 3) * sbot + (uint32_t)cg * 128 + (uint32_t)(f & 7) * 16;
+      *reinterpret_cast<uint4*>(Thi + off) = h;
+      *reinterpret_cast<uint4*>(Thi + vb + off) = l;
     }
-    if (*abort_flag) break;  // uniform: read after the chunk loop's last barrier
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    // 2. GEMM 1: hi.hi into [0, C), hi.lo + lo.hi into [C, 2C)
+    if (tid == 0) rtc_issue_gemm1(tmem, xhi_a, (uint32_t)xb, sbox, vhi_a, (uint32_t)vb, sbov, Tk, idesc1);
+    commit();
+    // while it runs: the next chunk's table and its rows in flight
+    int na = ca, nc0 = cc0;
+    advance(na, nc0);
+    if (na < ni) table(na, nc0, tb ^ 1);
+    __syncthreads();
+    if (na < ni) fetch(tb ^ 1);
+    wait();
+    // 3. Y~ = S o Y, split: hi over [0, C), lo over [C, 2C)
+    const uint32_t* sm = c_mask + tb * C;
+    const float* sw = c_w + tb * C;
+#pragma unroll 1
+    for (int j = 0; j < C; j += 16) {
+      uint32_t dh[16], dx[16];
+      tmem_ld16_nowait(tl + (uint32_t)j, dh);
+      tmem_ld16_nowait(tl + (uint32_t)(C + j), dx);
+      tmem_ld_wait();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float sc = ((sm[j + i] & vbits) == vbits) ? sw[j + i] : 0.f;
+        const float yv = __fmul_rn(__fadd_rn(__uint_as_float(dh[i]), __uint_as_float(dx[i])), sc);
+        dh[i] = tf32_rna(yv);
+        dx[i] = tf32_rna(__fsub_rn(yv, __uint_as_float(dh[i])));
+      }
+      tmem_st16(tl + (uint32_t)j, dh);
+      tmem_st16(tl + (uint32_t)(C + j), dx);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (*abort_flag) break;  // uniform
+    // 4. GEMM 2: K step s -> its own accumulator [2C + s TN, 2C + (s + 1) TN)
+    if (tid == 0) rtc_issue_gemm2(tmem, thi_a, (uint32_t)vb, sbot, TN, idesc2);
+    commit();
+    wait();
+    // 5. the K steps' sums into the accumulator ((s0 + s1) + (s2 + s3), then added)
+#pragma unroll
+    for (int f0 = 0; f0 < TN; f0 += 8) {
+      uint32_t r[KS2][8];
+#pragma unroll
+      for (int ks = 0; ks < KS2; ++ks) tmem_ld8_nowait(tl + (uint32_t)(2 * C + ks * TN + f0), r[ks]);
+      tmem_ld_wait();
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const float a01 = __fadd_rn(__uint_as_float(r[0][i]), __uint_as_float(r[1][i]));
+        const float a23 = __fadd_rn(__uint_as_float(r[2][i]), __uint_as_float(r[3][i]));
+        acc[f0 + i] = __fadd_rn(acc[f0 + i], __fadd_rn(a01, a23));
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();  // V, V^T, the raw rows and the TMEM columns are free for the next chunk
+    if (*abort_flag) break;
+    ca = na;
+    cc0 = nc0;
+    tb ^= 1;
   }
   __syncthreads();
   if (!*abort_flag && valid) {
@@ -440,7 +516,7 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
       double* hp = io.halo_out + (row - (long long)io.own_hi * g.ny * g.nz) * (T + 1);
 #pragma unroll
       for (int f = 0; f < TN; ++f)
-        if (f < T) hp[f] = acc[f];
+        if (f < T) hp[f] = (double)acc[f];
       hp[T] = wsum;
     } else {
       // out = m + A / wsum; a voxel no patch covers gets 0, as 0 / max(0, 1e-12)
@@ -450,8 +526,8 @@ __device__ __forceinline__ void recon_tc_body(const float* __restrict__ xc, cons
 #pragma unroll
       for (int f = 0; f < TN; f += 4)
         if (f < T)
-          op[f / 4] = make_float4((float)(mm + acc[f] * inv), (float)(mm + acc[f + 1] * inv),
-                                  (float)(mm + acc[f + 2] * inv), (float)(mm + acc[f + 3] * inv));
+          op[f / 4] = make_float4((float)(mm + (double)acc[f] * inv), (float)(mm + (double)acc[f + 1] * inv),
+                                  (float)(mm + (double)acc[f + 2] * inv), (float)(mm + (double)acc[f + 3] * inv));
     }
   }
   if (*abort_flag && tid == 0 && pend)  // let the MMAs in flight finish before the TMEM is released
