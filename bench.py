@@ -1088,16 +1088,20 @@ def serving_run(requests, rate, seed=0, duration=None, distinct=24, slots=4):
     idx = [i % k for i in range(len(arr))]
     P = sum(n_patches(vols[i].shape, shapes[i]["patch"], shapes[i]["stride"]) for i in idx)
     seq_s = sum(seq[i] for i in idx)
+    import collections
+
     with Server(n_slots=slots) as srv:
         start = time.perf_counter()
-        futs = []
+        pending = collections.deque()  # results are dropped as they arrive (host memory stays bounded)
         for t, i in zip(arr, idx):
             now = time.perf_counter() - start
             if t > now:
                 time.sleep(t - now)
-            futs.append(srv.submit(vols[i], shapes[i]["patch"], shapes[i]["stride"]))
-        for f in futs:
-            f.result()
+            pending.append(srv.submit(vols[i], shapes[i]["patch"], shapes[i]["stride"]))
+            while pending and pending[0].done():
+                pending.popleft().result()
+        while pending:
+            pending.popleft().result()
         st = srv.stats()
     return dict(value=st["patches_per_s"], unit="patches/s", p50_ms=st["p50_ms"], p99_ms=st["p99_ms"],
                 mean_ms=st["mean_ms"], requests=st["n"], requests_per_s=st["requests_per_s"],

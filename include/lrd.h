@@ -60,13 +60,18 @@ enum lrd_form {
    * running sums (out = m + sum w (x-m)P / sum w, float64 weight sums): error
    * against a float64 run of the algorithm at the float32 output floor. */
   LRD_FORM_ACCURATE = 1,
-  /* Precision form: the Gram contraction on the tcgen05 tensor cores in TF32
-   * with 3xTF32 split products (x = hi + lo; hi.hi + hi.lo + lo.hi) and FP32
-   * accumulation in tensor memory per plane (T <= 64, px*py <= 128; otherwise
-   * the FP32 Gram), near-tie MP decisions redone in FP64, the accurate
-   * form's accumulation. */
+  /* Precision form: both contractions on the tcgen05 tensor cores in TF32
+   * with 3xTF32 split products (x = hi + lo; hi.hi + hi.lo + lo.hi). The
+   * Gram accumulates in tensor memory per plane (T <= 64, px*py <= 128;
+   * otherwise the FP32 Gram); the reconstruction (T % 4 == 0, T <= 64) is two
+   * chained GEMMs per 4 x 4 x 8 voxel brick with one accumulator per 8
+   * columns, the mean kept out of the sums as in the accurate form.
+   * Near-tie MP decisions are redone in FP64. The tensor-core Gram's
+   * eigenvalues are about 1e-6 of the largest one from float64 (FP32 FFMA:
+   * about 1e-8), so a patch that close to an MP tie may take a different
+   * count than step 0. */
   LRD_FORM_TENSOR = 2,
-  /* Precision form with BF16 operands: as LRD_FORM_TENSOR, the Gram on
+  /* Precision form with BF16 Gram operands: as LRD_FORM_TENSOR, the Gram on
    * tcgen05 in kind::f16 with each float32 value split into three BF16 terms
    * (x = b0 + b1 + b2) and the six products of combined order <= 2 summed in
    * FP32 in tensor memory per plane. */
@@ -79,7 +84,13 @@ enum lrd_form {
  * the reconstruction brick (voxels per CTA along x, y, z) and threads per
  * voxel (recon_split: 1, 2 or 4); 0 = chosen by the plan's cost model (the
  * autotuner fills them in). These change speed only: every voxel's arithmetic
- * and accumulation order are the same for any brick and split. */
+ * and accumulation order are the same for any brick and split.
+ * ``gram_split``: threads sharing a 4x4 block of the column Gram (1, 2 or 4,
+ * each summing every n-th voxel row); ``eigh_block``: 1 = one warp per
+ * matrix (T <= 64), 2 = one CTA of 64 / 96 / 128 threads per matrix; 0 = the
+ * plan's choice for both. These two change the float32 rounding of the Gram
+ * and the eigenvalues (ranks stay the same: near-ties are decided in FP64
+ * from the input). */
 typedef struct lrd_problem {
   int32_t nx, ny, nz, nt;
   int32_t px, py, pz;
@@ -88,6 +99,8 @@ typedef struct lrd_problem {
   int32_t batch;
   int32_t brick_x, brick_y, brick_z;
   int32_t recon_split;
+  int32_t gram_split;
+  int32_t eigh_block;
 } lrd_problem;
 
 typedef struct lrd_plan lrd_plan;

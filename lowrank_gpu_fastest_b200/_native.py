@@ -68,7 +68,7 @@ class LrdProblem(ctypes.Structure):
 
     _fields_ = [(n, ctypes.c_int32) for n in
                 ("nx", "ny", "nz", "nt", "px", "py", "pz", "stride", "form", "batch",
-                 "brick_x", "brick_y", "brick_z", "recon_split")]
+                 "brick_x", "brick_y", "brick_z", "recon_split", "gram_split", "eigh_block")]
 
 
 class LrdError(RuntimeError):
@@ -107,14 +107,15 @@ def check(rc: int):
         raise LrdError(rc, msg)
 
 
-def make_problem(shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0):
+def make_problem(shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0, gram_split=0,
+                 eigh_block=0):
     if form not in FORMS:
         raise ValueError(f"form must be one of {sorted(FORMS)}, got {form!r}")
     nx, ny, nz, nt = (int(s) for s in shape)
     px, py, pz = (int(p) for p in patch)
     bx, by, bz = (int(b) for b in (brick or (0, 0, 0)))
     return LrdProblem(nx, ny, nz, nt, px, py, pz, int(stride), FORMS[form], int(batch or 0),
-                      bx, by, bz, int(split or 0))
+                      bx, by, bz, int(split or 0), int(gram_split or 0), int(eigh_block or 0))
 
 
 def selftest_wait_timeout(limit_ns: int, d_status: int, stream: int):
@@ -138,9 +139,9 @@ class Plan:
     """Owns an ``lrd_plan*`` for one problem on the current CUDA device."""
 
     def __init__(self, shape, patch=(11, 11, 11), stride=3, form="plain", batch=0, brick=None, split=0,
-                 _slab=None):
+                 _slab=None, gram_split=0, eigh_block=0):
         lib = load()
-        self.problem = make_problem(shape, patch, stride, form, batch, brick, split)
+        self.problem = make_problem(shape, patch, stride, form, batch, brick, split, gram_split, eigh_block)
         nx, ny, nz, nt = (int(s) for s in shape)
         self.shape = (nx, ny, nz, nt)
         self.patch = tuple(int(p) for p in patch)
@@ -229,7 +230,7 @@ class BatchPlan:
 
     def __init__(self, problems, n_streams=4):
         """``problems``: list of dicts with shape, patch, stride, form, batch,
-        brick, split (the last four optional)."""
+        brick, split, gram_split, eigh_block (all but shape optional)."""
         lib = load()
         arr = (LrdProblem * len(problems))()
         for i, pr in enumerate(problems):
@@ -238,7 +239,8 @@ class BatchPlan:
             bx, by, bz = (int(v) for v in (pr.get("brick") or (0, 0, 0)))
             arr[i] = LrdProblem(nx, ny, nz, nt, px, py, pz, int(pr.get("stride", 3)),
                                 FORMS[pr.get("form", "plain")], int(pr.get("batch") or 0), bx, by, bz,
-                                int(pr.get("split") or 0))
+                                int(pr.get("split") or 0), int(pr.get("gram_split") or 0),
+                                int(pr.get("eigh_block") or 0))
         self._arr = arr
         self.n = len(problems)
         h = ctypes.c_void_p()

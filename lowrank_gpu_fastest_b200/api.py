@@ -30,14 +30,15 @@ _workspaces: dict = {}
 _lock = threading.Lock()
 
 
-def _plan(shape, patch, stride, form, batch, device, brick=None, split=0):
+def _plan(shape, patch, stride, form, batch, device, brick=None, split=0, gram_split=0, eigh_block=0):
     key = (tuple(shape), tuple(patch), int(stride), form, int(batch or 0), device,
-           tuple(brick) if brick else None, int(split or 0))
+           tuple(brick) if brick else None, int(split or 0), int(gram_split or 0), int(eigh_block or 0))
     with _lock:
         p = _plans.get(key)
         if p is None:
             with torch.cuda.device(device):
-                p = _native.Plan(shape, patch, stride, form, batch or 0, brick, split)
+                p = _native.Plan(shape, patch, stride, form, batch or 0, brick, split, gram_split=gram_split,
+                                 eigh_block=eigh_block)
             _plans[key] = p
     return p
 
@@ -53,11 +54,14 @@ def _workspace(plan, device, stream):
 
 
 def get_plan(shape, patch=(11, 11, 11), stride=3, form="plain", batch=None, device=None, brick=None,
-             split=0):
-    """The cached native plan for a problem (creates it on first use)."""
+             split=0, gram_split=0, eigh_block=0):
+    """The cached native plan for a problem (creates it on first use). The
+    launch-shape arguments (brick, split, gram_split, eigh_block) default to
+    the plan's own choices; :func:`lowrank_gpu_fastest_b200.tune.tune` picks
+    them by timing."""
     if device is None:
         device = torch.cuda.current_device()
-    return _plan(shape, patch, stride, form, batch, device, brick, split)
+    return _plan(shape, patch, stride, form, batch, device, brick, split, gram_split, eigh_block)
 
 
 def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", return_ranks=False,
@@ -68,9 +72,10 @@ def denoise(vol, patch=(11, 11, 11), stride=3, batch=None, *, form="plain", retu
     (common.py:29), ``batch`` = patches per Gram/eigensolver launch
     (step8_tuned.py:21; ``None`` = all). ``form`` is ``"plain"`` (float32,
     step-0 accumulation order), ``"accurate"`` (float64 accumulation, close
-    to the float64 run), ``"tensor"`` (as accurate, the Gram on the tensor
-    cores in split TF32) or ``"tensor_bf16"`` (as tensor, with three-term
-    BF16 split products). With ``return_ranks`` the per-patch MP ranks
+    to the float64 run), ``"tensor"`` (the Gram and the reconstruction on the
+    tensor cores in split TF32, the mean kept out of the sums as in accurate)
+    or ``"tensor_bf16"`` (as tensor, the Gram with three-term BF16 split
+    products). With ``return_ranks`` the per-patch MP ranks
     (x-major patch order) are returned too. ``out`` (CUDA input only): a
     preallocated output tensor of the volume's shape.
     """
@@ -166,8 +171,9 @@ def denoise_batch(vols, patches=(11, 11, 11), strides=3, *, form="plain", use_gr
     (``lrd_batch_*``; ``n_streams`` is kept for compatibility and unused);
     with ``use_graph`` the whole batch is one CUDA-graph launch, captured on
     the first call with these buffers. With
-    ``autotune`` each distinct (frames, patch, stride) gets its reconstruction
-    launch shape from :func:`lowrank_gpu_fastest_b200.tune.tune`.
+    ``autotune`` each distinct (frames, patch, stride) gets its launch shapes
+    (reconstruction brick and split, Gram split, eigensolver schedule) from
+    :func:`lowrank_gpu_fastest_b200.tune.tune`.
     """
     if not torch.cuda.is_available():
         raise RuntimeError("denoise_batch needs a CUDA device")
@@ -196,11 +202,11 @@ def denoise_batch(vols, patches=(11, 11, 11), strides=3, *, form="plain", use_gr
         if autotune:
             from .tune import tune
 
-            brick, split = tune(tuple(v.shape), p, int(s), form, device)
-            pr["brick"], pr["split"] = brick, split
+            pr.update(tune(tuple(v.shape), p, int(s), form, device))
         problems.append(pr)
     key = (device, int(n_streams), tuple((pr["shape"], pr["patch"], pr["stride"], pr["form"],
-                                          tuple(pr.get("brick") or ()), pr.get("split", 0)) for pr in problems))
+                                          tuple(pr.get("brick") or ()), pr.get("split", 0), pr.get("gram_split", 0),
+                                          pr.get("eigh_block", 0)) for pr in problems))
     with _lock:
         bp = _batch_plans.get(key)
         if bp is None:

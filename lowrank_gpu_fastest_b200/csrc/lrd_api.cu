@@ -81,6 +81,7 @@ struct lrd_plan {
   size_t smem_gramtc;
   int gramz_ring;          // window accumulator slots
   int gramz_ks = 1;        // voxel-row split per 4x4 Gram block (threads per block)
+  bool eigh_cta = false;   // eigensolver: one CTA per matrix (else one warp)
   size_t smem_gramz;
   int gramz_slots = 0;     // column CTAs resident at once on the device (0: never cut columns)
   int gramtc_slots = 0;    // the same for the tensor-core column Gram
@@ -231,21 +232,30 @@ void choose_brick(const int dims[3], const int pat[3], const std::vector<int32_t
       }
 }
 
-// Float32 eigensolver kernel and its shared-memory floats for frame count T:
-// the register-resident kernel up to T = 64, the shared-memory one above.
-size_t eigh_smem_for(int T) {
+// Float32 eigensolver kernel, its threads and shared-memory floats for frame
+// count T: one warp per matrix (register-resident rows) up to T = 64, one
+// CTA of TMAX threads per matrix (TMAX = 64, 96, 128) above or when asked.
+bool eigh_use_cta(int T, int eigh_block) { return eigh_block == 2 || (eigh_block == 0 && T > 64); }
+size_t eigh_smem_for(int T, bool cta) {
+  if (cta) {
+    if (T <= 64) return lrd::eigh_cta_smem_floats<64>();
+    if (T <= 96) return lrd::eigh_cta_smem_floats<96>();
+    return lrd::eigh_cta_smem_floats<128>();
+  }
   if (T <= 32) return lrd::eigh_reg_smem_floats<32>();
   if (T <= 48) return lrd::eigh_reg_smem_floats<48>();
-  if (T <= 64) return lrd::eigh_reg_smem_floats<64>();
-  if (T <= 96) return lrd::eigh_cta_smem_floats<96>();
-  return lrd::eigh_cta_smem_floats<128>();
+  return lrd::eigh_reg_smem_floats<64>();
 }
-const void* eigh_kernel_for(int T) {
+const void* eigh_kernel_for(int T, bool cta, unsigned* threads = nullptr) {
+  if (threads) *threads = cta ? (T <= 64 ? 64u : (T <= 96 ? 96u : 128u)) : 32u;
+  if (cta) {
+    if (T <= 64) return (const void*)lrd::eigh_cta_kernel<64>;
+    if (T <= 96) return (const void*)lrd::eigh_cta_kernel<96>;
+    return (const void*)lrd::eigh_cta_kernel<128>;
+  }
   if (T <= 32) return (const void*)lrd::eigh_reg_kernel<32>;
   if (T <= 48) return (const void*)lrd::eigh_reg_kernel<48>;
-  if (T <= 64) return (const void*)lrd::eigh_reg_kernel<64>;
-  if (T <= 96) return (const void*)lrd::eigh_cta_kernel<96>;
-  return (const void*)lrd::eigh_cta_kernel<128>;
+  return (const void*)lrd::eigh_reg_kernel<64>;
 }
 
 template <int TPT, int SPLIT>
@@ -481,21 +491,14 @@ int run_eigh(const lrd_plan* P, char* ws, const float* d_gram, float* d_vecs, fl
     float* w = d_wgt + p0;
     float* s2 = sig2 + p0;
     const int nv = P->g.nvox_patch;
-    if (T <= 32)
-      lrd::eigh_reg_kernel<32><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
-                                                                        rids);
-    else if (T <= 48)
-      lrd::eigh_reg_kernel<48><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
-                                                                        rids);
-    else if (T <= 64)
-      lrd::eigh_reg_kernel<64><<<(unsigned)nb, 32, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
-                                                                        rids);
-    else if (T <= 96)
-      lrd::eigh_cta_kernel<96><<<(unsigned)nb, 96, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0, rcount,
-                                                                       rids);
-    else
-      lrd::eigh_cta_kernel<128><<<(unsigned)nb, 128, P->smem_eigh, st>>>(gin, vout, lout, r, w, s2, T, nv, p0,
-                                                                         rcount, rids);
+    unsigned eth = 32;
+    const void* efn = eigh_kernel_for(T, P->eigh_cta, &eth);
+    long long p0v = p0;
+    int tv = T, nvv = nv;
+    void* eargs[] = {(void*)&gin, (void*)&vout, (void*)&lout, (void*)&r,      (void*)&w,   (void*)&s2,
+                     (void*)&tv,  (void*)&nvv,  (void*)&p0v,  (void*)&rcount, (void*)&rids};
+    cudaError_t le = cudaLaunchKernel(efn, dim3((unsigned)nb), dim3(eth), eargs, P->smem_eigh, st);
+    if (le != cudaSuccess) return cuda_fail(le, "eigh kernel launch");
     int rc = launch_check("eigh kernel launch");
     if (rc) return rc;
   }
@@ -571,6 +574,12 @@ int validate_problem(const lrd_problem* pr) {
   if (pr->batch < 0) return fail(LRD_ERR_INVALID, "batch must be >= 0, got %d", pr->batch);
   if (pr->recon_split != 0 && pr->recon_split != 1 && pr->recon_split != 2 && pr->recon_split != 4)
     return fail(LRD_ERR_INVALID, "recon_split must be 0, 1, 2 or 4, got %d", pr->recon_split);
+  if (pr->gram_split != 0 && pr->gram_split != 1 && pr->gram_split != 2 && pr->gram_split != 4)
+    return fail(LRD_ERR_INVALID, "gram_split must be 0, 1, 2 or 4, got %d", pr->gram_split);
+  if (pr->eigh_block < 0 || pr->eigh_block > 2)
+    return fail(LRD_ERR_INVALID, "eigh_block must be 0 (plan), 1 (warp) or 2 (CTA), got %d", pr->eigh_block);
+  if (pr->eigh_block == 1 && pr->nt > 64)
+    return fail(LRD_ERR_INVALID, "eigh_block 1 (one warp per matrix) needs T <= 64, got T = %d", pr->nt);
   const long long nvox = (long long)pr->nx * pr->ny * pr->nz;
   if (nvox * pr->nt >= (1LL << 40)) return fail(LRD_ERR_UNSUPPORTED, "volume too large");
   const long long nvp = (long long)pr->px * pr->py * pr->pz;
@@ -769,13 +778,14 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   P->center_warps = 4;
   P->smem_center = sizeof(float) * (size_t)P->center_warps * (32 * (T + 1) + 32);
   P->smem_gram = sizeof(float) * (size_t)pr->py * pr->pz * (4 * nb4);
-  P->smem_eigh = sizeof(float) * eigh_smem_for(T);
+  P->eigh_cta = eigh_use_cta(T, pr->eigh_block);
+  P->smem_eigh = sizeof(float) * eigh_smem_for(T, P->eigh_cta);
   P->smem_recon = lrd::recon_smem_bytes(T, max_touch(brick));
   {
     int ring = 1;
     for (int z = 0; z < pr->nz; ++z) ring = std::max(ring, cover[2][2 * z + 1] - cover[2][2 * z] + 1);
     P->gramz_ring = ring;
-    P->gramz_ks = gramz_split(T);
+    P->gramz_ks = pr->gram_split > 0 ? pr->gram_split : gramz_split(T);
     P->smem_gramz = lrd::gramz_smem_bytes(pr->px * pr->py, T, ring, P->gram_threads);
     P->use_gramz = (T % 4 == 0) && P->smem_gramz <= 200 * 1024 && tensor_map_encoder() != nullptr &&
                    pr->px <= 256 && pr->py <= 256;
@@ -812,7 +822,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
         (void)cudaGetLastError();
     }
   }
-  if (!rc) rc = set_smem(eigh_kernel_for(T), P->smem_eigh);
+  if (!rc) rc = set_smem(eigh_kernel_for(T, P->eigh_cta), P->smem_eigh);
   if (!rc && !P->recon_tc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, false), P->smem_recon);
   if (!rc && !P->recon_tc) rc = set_smem(recon_kernel_ptr(P->tpt, P->split, true), P->smem_recon);
   if (!rc && P->recon_tc) rc = set_smem(recon_tc_ptr(T), P->smem_recon_tc);

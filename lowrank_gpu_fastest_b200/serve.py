@@ -9,8 +9,10 @@ owns the device:
   workspace) fits in the HBM that ``cudaMemGetInfo`` reports free minus a
   reserve; requests that do not fit wait, in arrival order, while others run;
 * each admitted request runs on its slot's stream: host->device copy from a
-  pinned staging buffer, ``lrd_denoise``, device->host copy into pinned
-  memory, an event; requests on different slots overlap on the device;
+  pinned staging buffer (filled at admission, so only admitted requests hold
+  pinned host memory and a long backlog holds no more than the callers'
+  arrays), ``lrd_denoise``, device->host copy into pinned memory, an event;
+  requests on different slots overlap on the device;
 * completion - the scheduler polls the events without blocking, resolves the
   future with the denoised volume (and ranks), frees the slot, returns the
   request's device buffers to a pool (reused by later requests of the same
@@ -150,9 +152,9 @@ class Server:
         except Exception as e:  # a bad request fails its own future only
             fut.set_exception(e)
             return fut
-        # staged into pinned memory on the caller's thread, off the scheduler
-        h_in = self.torch.from_numpy(vol).pin_memory()
-        r = _Req(vol, h_in, tuple(int(p) for p in patch), int(stride), form, t_submit, fut)
+        # staged into pinned memory at admission: a backlog of waiting requests
+        # holds only the callers' arrays
+        r = _Req(vol, None, tuple(int(p) for p in patch), int(stride), form, t_submit, fut)
         r.n_patches = npatch
         with self._lock:
             self._pending.append(r)
@@ -190,8 +192,7 @@ class Server:
             return {}
         from .tune import tune
 
-        brick, split = tune(r.vol.shape, r.patch, r.stride, r.form, self.device)
-        return dict(brick=brick, split=split)
+        return tune(r.vol.shape, r.patch, r.stride, r.form, self.device)
 
     def _fits(self, need):
         free, _ = self.torch.cuda.mem_get_info(self.device)
@@ -232,6 +233,7 @@ class Server:
             self._in_flight_bytes += need
             st = self._streams[slot]
             dev = f"cuda:{self.device}"
+            r.h_in = torch.from_numpy(r.vol).pin_memory()
             with torch.cuda.device(self.device), torch.cuda.stream(st):
                 h_in = r.h_in
                 vbytes, rbytes = r.vol.nbytes, 4 * r.n_patches

@@ -1,18 +1,23 @@
-"""Autotuner for the reconstruction launch shape (brick and threads per voxel).
+"""Autotuner for the launch shapes of a problem: the reconstruction's brick
+and threads per voxel, the column Gram's voxel-row split, and the
+eigensolver's matrix-per-warp or matrix-per-CTA schedule.
 
-Brick (0, 0, 0) with split 0 is the plan's own choice: the warp kernel (one
-warp per 2x2x2 voxel block) for the frame counts it is built for, else the
-brick kernel with the cost model's brick.
+Brick (0, 0, 0) with split 0, gram_split 0 and eigh_block 0 are the plan's
+own choices: the warp kernel (one warp per 2x2x2 voxel block) for the frame
+counts it is built for, else the brick kernel with the cost model's brick;
+the Gram split measured best per frame count; one warp per matrix up to
+T = 64.
 
-The reconstruction kernel's speed depends on the brick of voxels a CTA owns
-(how many of the patches touching the brick actually cover each voxel, how
-many CTAs fit on an SM) and on how many threads share a voxel's frames. The
-plan's cost model picks a default; this module times a small candidate set on
-the current GPU with a synthetic volume of the problem's shape and keeps the
-fastest. Results are cached per (GPU architecture, frames, patch, stride, form)
-in a JSON file (``LRD_TUNE_CACHE``, default
-``~/.cache/lowrank_gpu_fastest_b200/tune.json``). Every candidate gives
-bit-identical output - only the time differs.
+Each phase is tuned on its own phase time (the library's phase events, mean
+of ``reps`` warm calls) on a synthetic volume of the problem's shape: first
+the reconstruction over a candidate set of bricks and splits, then the Gram
+split over 1, 2, 4 (column Gram only), then the eigensolver schedule (T <= 64:
+warp or CTA). Results are cached per (GPU architecture, frames, patch,
+stride, form) in a JSON file (``LRD_TUNE_CACHE``, default
+``~/.cache/lowrank_gpu_fastest_b200/tune.json``). The reconstruction choices
+give bit-identical output; the Gram split and the eigensolver schedule
+change the float32 rounding of the Gram and the eigenvalues (the ranks stay
+the same: near-ties are decided in float64 from the input).
 """
 
 from __future__ import annotations
@@ -56,7 +61,12 @@ def _save(d):
 
 
 def key(arch: str, T: int, patch, stride: int, form: str) -> str:
-    return f"{arch}|T{T}|p{'x'.join(str(int(v)) for v in patch)}|s{int(stride)}|{form}"
+    return f"v2|{arch}|T{T}|p{'x'.join(str(int(v)) for v in patch)}|s{int(stride)}|{form}"
+
+
+def _choice(d) -> dict:
+    return dict(brick=tuple(int(v) for v in d["brick"]), split=int(d["split"]),
+                gram_split=int(d.get("gram_split", 0)), eigh_block=int(d.get("eigh_block", 0)))
 
 
 def candidates(T: int, patch, stride: int):
@@ -76,11 +86,12 @@ def candidates(T: int, patch, stride: int):
 
 def tune(shape, patch=(11, 11, 11), stride=3, form="plain", device=None, max_candidates=24, reps=3,
          force=False):
-    """Best ``(brick, split)`` for the problem on the current GPU (cached).
+    """Best launch shapes for the problem on the current GPU (cached): a dict
+    with ``brick``, ``split``, ``gram_split`` and ``eigh_block`` (the keyword
+    arguments of :func:`lowrank_gpu_fastest_b200.api.get_plan`).
 
-    Candidates are ranked by a proxy first (thread-slots of the brick, as the
-    plan's model) and the ``max_candidates`` best are timed by the library's
-    phase events (reconstruction phase, mean of ``reps`` warm calls).
+    Reconstruction candidates are ranked by a proxy first (thread-slots of
+    the brick, as the plan's model) and the ``max_candidates`` best are timed.
     """
     import torch
 
@@ -97,12 +108,11 @@ def tune(shape, patch=(11, 11, 11), stride=3, form="plain", device=None, max_can
     with _lock:
         if not force:
             if k in _mem:
-                return _mem[k]
+                return dict(_mem[k])
             disk = _load()
             if k in disk:
-                v = disk[k]
-                _mem[k] = (tuple(v["brick"]), int(v["split"]))
-                return _mem[k]
+                _mem[k] = _choice(disk[k])
+                return dict(_mem[k])
 
     def slots(b):
         tot = 1.0
@@ -122,38 +132,66 @@ def tune(shape, patch=(11, 11, 11), stride=3, form="plain", device=None, max_can
     # kernel where it is built for T, else the cost model's brick)
     cands = [((0, 0, 0), 0)] + cands[:max_candidates]
     vol, _ = make_phantom_lowrank(tuple(int(v) for v in shape), seed=7)
-    best, best_ms, results = None, float("inf"), []
+    timed = {"recon": [], "gram": [], "eigh_mp": []}
     with torch.cuda.device(device):
         d = torch.from_numpy(vol).cuda()
         out = torch.empty_like(d)
         s = torch.cuda.current_stream().cuda_stream
-        ws = None
-        for brick, split in cands:
+        ws = [None]
+
+        def phase_ms(phase, brick, split, gram_split=0, eigh_block=0):
             try:
-                plan = _native.Plan(shape, patch, stride, form, 0, brick, split)
+                plan = _native.Plan(shape, patch, stride, form, 0, brick, split, gram_split=gram_split,
+                                    eigh_block=eigh_block)
             except _native.LrdError:
-                continue
-            if ws is None or ws.numel() < plan.workspace_bytes:
-                ws = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=d.device)
-            plan.denoise(d.data_ptr(), out.data_ptr(), None, ws.data_ptr(), s)
+                return None
+            if ws[0] is None or ws[0].numel() < plan.workspace_bytes:
+                ws[0] = torch.empty(plan.workspace_bytes, dtype=torch.uint8, device=d.device)
+            plan.denoise(d.data_ptr(), out.data_ptr(), None, ws[0].data_ptr(), s)
             plan.set_profiling(True)
             for _ in range(reps):
-                plan.denoise(d.data_ptr(), out.data_ptr(), None, ws.data_ptr(), s)
+                plan.denoise(d.data_ptr(), out.data_ptr(), None, ws[0].data_ptr(), s)
             ph, n = plan.phase_ms()
             plan.set_profiling(False)
-            ms = ph["recon"] / max(n, 1)
-            results.append((brick, split, ms))
+            return ph[phase] / max(n, 1)
+
+        best = None
+        best_ms = float("inf")
+        for brick, split in cands:  # reconstruction
+            ms = phase_ms("recon", brick, split)
+            if ms is None:
+                continue
+            timed["recon"].append([list(brick), split, round(ms, 4)])
             if ms < best_ms:
                 best, best_ms = (tuple(brick), int(split)), ms
-    if best is None:
-        raise RuntimeError("autotuner: no candidate plan could be created")
+        if best is None:
+            raise RuntimeError("autotuner: no candidate plan could be created")
+        choice = dict(brick=best[0], split=best[1], gram_split=0, eigh_block=0)
+        best_gram = (None, float("inf"))
+        for gs in (1, 2, 4):  # column-Gram voxel-row split
+            ms = phase_ms("gram", best[0], best[1], gram_split=gs)
+            if ms is not None:
+                timed["gram"].append([gs, round(ms, 4)])
+                if ms < best_gram[1]:
+                    best_gram = (gs, ms)
+        if best_gram[0] is not None:
+            choice["gram_split"] = best_gram[0]
+        best_eigh = (None, float("inf"))
+        for eb in ((1, 2) if T <= 64 else (2,)):  # eigensolver: warp or CTA per matrix
+            ms = phase_ms("eigh_mp", best[0], best[1], gram_split=choice["gram_split"], eigh_block=eb)
+            if ms is not None:
+                timed["eigh_mp"].append([eb, round(ms, 4)])
+                if ms < best_eigh[1]:
+                    best_eigh = (eb, ms)
+        if best_eigh[0] is not None:
+            choice["eigh_block"] = best_eigh[0]
     with _lock:
-        _mem[k] = best
+        _mem[k] = dict(choice)
         disk = _load()
-        disk[k] = {"brick": list(best[0]), "split": best[1], "recon_ms": best_ms,
-                   "timed": [[list(b), sp, round(ms, 4)] for b, sp, ms in results]}
+        disk[k] = {"brick": list(choice["brick"]), "split": choice["split"], "gram_split": choice["gram_split"],
+                   "eigh_block": choice["eigh_block"], "recon_ms": best_ms, "timed": timed}
         _save(disk)
-    return best
+    return dict(choice)
 
 
 def clear_memory_cache():

@@ -54,6 +54,9 @@ def test_null_arguments_rejected(lib):
     ((16, 16, 16, 48, 5, 5, 5, 2, 0, -1), _native.LRD_ERR_INVALID),    # negative batch
     ((16, 16, 16, 200, 7, 7, 7, 2, 0, 0), _native.LRD_ERR_UNSUPPORTED),  # T above the compiled limit
     ((16, 16, 16, 48, 3, 3, 3, 2, 0, 0), _native.LRD_ERR_UNSUPPORTED),   # N = 27 < T
+    ((16, 16, 16, 48, 5, 5, 5, 2, 0, 0, 0, 0, 0, 0, 3, 0), _native.LRD_ERR_INVALID),  # Gram split 3
+    ((16, 16, 16, 48, 5, 5, 5, 2, 0, 0, 0, 0, 0, 0, 0, 3), _native.LRD_ERR_INVALID),  # eigh_block 3
+    ((16, 16, 16, 80, 7, 7, 7, 2, 0, 0, 0, 0, 0, 0, 0, 1), _native.LRD_ERR_INVALID),  # warp per matrix at T = 80
 ])
 def test_invalid_problems_rejected_before_device(lib, fields, code):
     pr = _native.LrdProblem(*fields)
