@@ -35,6 +35,8 @@ __device__ long long* g_phase_clocks;  // 8 stamps per block, set by a probe bui
   do { } while (0)
 #endif
 
+constexpr int kInvSolves = 2;  // inverse-iteration solves per eigenvector
+
 template <int TMAX>
 __host__ __device__ constexpr int eigh_reg_nr() {
   return (TMAX + 31) / 32;
@@ -412,7 +414,12 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
       // the vector in shared memory (Yt column q)
       float* Y = Yt;
       for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
-      for (int iter = 0; iter < 3; ++iter) {
+      // two solves: the shift is the eigenvalue to eps ||T||, so each solve
+      // shrinks the other eigenvectors' share by about eps ||T|| / gap; with
+      // pivots clamped at eps ||T|| the vector grows at most ~1e7-fold per
+      // solve (well inside float32 range), so it is scaled only once, after
+      // the last solve
+      for (int iter = 0; iter < kInvSolves; ++iter) {
         for (int i = 0; i < n - 1; ++i) {
           const float yi = Y[i * kLdy + q], yn = Y[(i + 1) * kLdy + q];
           const float m = ML[i * kInvGroup + q];
@@ -440,6 +447,7 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
           for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
           continue;
         }
+        if (iter + 1 < kInvSolves) continue;
         const float sa = 1.f / amax;
         float nrm = 0.f;
         for (int i = 0; i < n; ++i) {
