@@ -94,6 +94,7 @@ __device__ __forceinline__ float start_entry(int i, int j) {
 }
 
 constexpr int kInvGroup = 8;  // eigenvectors refined concurrently (one lane each)
+constexpr int kInvSolves = 2;  // float32 solvers: inverse-iteration solves per eigenvector
 
 // Floats of the packed Householder reflector rows of the float32 solvers: row
 // k (k < n - 2 <= TMAX - 2) is stored from its first live 4-column group on,

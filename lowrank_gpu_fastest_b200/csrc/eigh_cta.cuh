@@ -319,7 +319,9 @@ __device__ __forceinline__ void eigh_cta_body(const float* gram, float* vecs, fl
       // fully unrolled loops measured slower (104 K vs 66 K cycles per matrix)
       float* Y = Yt;
       for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
-      for (int iter = 0; iter < 3; ++iter) {
+      // two solves, rescaled in between only when grown past 1e15 (as the
+      // one-warp solver)
+      for (int iter = 0; iter < kInvSolves; ++iter) {
         for (int i = 0; i < n - 1; ++i) {
           const float yi = Y[i * kLdy + q], yn = Y[(i + 1) * kLdy + q];
           const float m = ML[i * kInvGroup + q];
@@ -347,6 +349,7 @@ __device__ __forceinline__ void eigh_cta_body(const float* gram, float* vecs, fl
           for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
           continue;
         }
+        if (iter + 1 < kInvSolves && amax < 1e15f) continue;
         const float sa = 1.f / amax;
         float nrm = 0.f;
         for (int i = 0; i < n; ++i) {

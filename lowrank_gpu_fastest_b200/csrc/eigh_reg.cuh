@@ -35,8 +35,6 @@ __device__ long long* g_phase_clocks;  // 8 stamps per block, set by a probe bui
   do { } while (0)
 #endif
 
-constexpr int kInvSolves = 2;  // inverse-iteration solves per eigenvector
-
 template <int TMAX>
 __host__ __device__ constexpr int eigh_reg_nr() {
   return (TMAX + 31) / 32;
@@ -48,6 +46,56 @@ __host__ __device__ constexpr int eigh_reg_nr() {
 template <int TMAX>
 __host__ __device__ constexpr size_t eigh_reg_smem_floats() {
   return eigh_hv_floats<TMAX>() + 5 * TMAX + (size_t)3 * TMAX * kInvGroup + (size_t)TMAX * kLdy;
+}
+
+template <int V>
+struct IntTag {
+  static constexpr int value = V;
+};
+
+// Sums of G = 4 or 8 values over the warp, every lane getting all G sums:
+// halving exchanges (each lane keeps half of its values and adds its
+// partner's copies of them: G/2 + G/4 + ... shuffles) until a lane holds one
+// value summed over 8 (G = 8) or 16 (G = 4) lanes, two or one more xor steps
+// finish it over the warp, then G broadcasts - G + 8 shuffles for G = 8
+// against 5 G for a butterfly per value.
+template <int G>
+__device__ __forceinline__ void warp_allsum(float (&v)[G]) {
+  static_assert(G == 4 || G == 8, "4 or 8 values");
+  const int lane = threadIdx.x & 31;
+  const bool b4 = (lane >> 4) & 1, b3 = (lane >> 3) & 1, b2 = (lane >> 2) & 1;
+  float w;
+  if constexpr (G == 8) {
+    float w4[4], w2[2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float keep = b4 ? v[i + 4] : v[i], send = b4 ? v[i] : v[i + 4];
+      w4[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float keep = b3 ? w4[i + 2] : w4[i], send = b3 ? w4[i] : w4[i + 2];
+      w2[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const float keep = b2 ? w2[1] : w2[0], send = b2 ? w2[0] : w2[1];
+    w = keep + __shfl_xor_sync(0xffffffffu, send, 4);  // value 4 b4 + 2 b3 + b2
+  } else {
+    float w2[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const float keep = b4 ? v[i + 2] : v[i], send = b4 ? v[i] : v[i + 2];
+      w2[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    const float keep = b3 ? w2[1] : w2[0], send = b3 ? w2[0] : w2[1];
+    w = keep + __shfl_xor_sync(0xffffffffu, send, 8);  // value 2 b4 + b3
+    w += __shfl_xor_sync(0xffffffffu, w, 4);
+  }
+  w += __shfl_xor_sync(0xffffffffu, w, 2);
+  w += __shfl_xor_sync(0xffffffffu, w, 1);
+#pragma unroll
+  for (int q = 0; q < G; ++q)  // value q sits in lane (q's bits spread to lane bits 4, 3, 2 / 4, 3)
+    v[q] = __shfl_sync(0xffffffffu, w, G == 8 ? (((q & 4) << 2) | ((q & 2) << 2) | ((q & 1) << 2))
+                                              : (((q & 2) << 3) | ((q & 1) << 3)));
 }
 
 // Sturm counts (eigenvalues below x0 and x1) of the tridiagonal held in
@@ -415,10 +463,10 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
       float* Y = Yt;
       for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j);
       // two solves: the shift is the eigenvalue to eps ||T||, so each solve
-      // shrinks the other eigenvectors' share by about eps ||T|| / gap; with
-      // pivots clamped at eps ||T|| the vector grows at most ~1e7-fold per
-      // solve (well inside float32 range), so it is scaled only once, after
-      // the last solve
+      // shrinks the other eigenvectors' share by about eps ||T|| / gap; a
+      // solve grows the vector by about 1 / (eps ||T||) per eigenvalue that
+      // close to the shift, so it is rescaled between solves only when it has
+      // grown past 1e15, and normalised after the last one
       for (int iter = 0; iter < kInvSolves; ++iter) {
         for (int i = 0; i < n - 1; ++i) {
           const float yi = Y[i * kLdy + q], yn = Y[(i + 1) * kLdy + q];
@@ -447,7 +495,7 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
           for (int i = 0; i < n; ++i) Y[i * kLdy + q] = start_entry(i, j + 977 * (iter + 1));
           continue;
         }
-        if (iter + 1 < kInvSolves) continue;
+        if (iter + 1 < kInvSolves && amax < 1e15f) continue;  // rescale only a vector grown this far
         const float sa = 1.f / amax;
         float nrm = 0.f;
         for (int i = 0; i < n; ++i) {
@@ -469,39 +517,44 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
 #pragma unroll
       for (int q = 0; q < kInvGroup; ++q) yr[ri][q] = (r < n && q < g) ? Yt[r * kLdy + q] : 0.f;
     }
-    // back-transform x = H(0) ... H(n-3) y
-    int hb = hbase;  // end of the packed rows
-    for (int k = n - 3; k >= 0; --k) {
-      const int j4lo = (k + 1) >> 2;
-      hb -= TMAX - 4 * j4lo;
-      const float tk = tau[k];
-      if (tk == 0.f) continue;
-      const float* hrow = HV + hb - 4 * j4lo;
-      float hr[NR];
+    // back-transform x = H(0) ... H(n-3) y, on the first G = 4 or 8 vectors
+    // of the chunk (G >= g)
+    auto back_transform = [&](auto gtag) {
+      constexpr int G = decltype(gtag)::value;
+      int hb = hbase;  // end of the packed rows
+      for (int k = n - 3; k >= 0; --k) {
+        const int j4lo = (k + 1) >> 2;
+        hb -= TMAX - 4 * j4lo;
+        const float tk = tau[k];
+        if (tk == 0.f) continue;
+        const float* hrow = HV + hb - 4 * j4lo;
+        float hr[NR];
 #pragma unroll
-      for (int ri = 0; ri < NR; ++ri) {
-        const int r = lane + 32 * ri;
-        hr[ri] = (r >= 4 * j4lo && r < n) ? hrow[r] : 0.f;
+        for (int ri = 0; ri < NR; ++ri) {
+          const int r = lane + 32 * ri;
+          hr[ri] = (r >= 4 * j4lo && r < n) ? hrow[r] : 0.f;
+        }
+        float dq[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          float s_ = 0.f;
+#pragma unroll
+          for (int ri = 0; ri < NR; ++ri) s_ = fmaf(hr[ri], yr[ri][q], s_);
+          dq[q] = s_;
+        }
+        warp_allsum<G>(dq);
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+          const float f = tk * dq[q];
+#pragma unroll
+          for (int ri = 0; ri < NR; ++ri) yr[ri][q] = fmaf(-f, hr[ri], yr[ri][q]);
+        }
       }
-      float dq[kInvGroup];
-#pragma unroll
-      for (int q = 0; q < kInvGroup; ++q) {
-        float s_ = 0.f;
-#pragma unroll
-        for (int ri = 0; ri < NR; ++ri) s_ = fmaf(hr[ri], yr[ri][q], s_);
-        dq[q] = s_;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-        for (int q = 0; q < kInvGroup; ++q) dq[q] += __shfl_xor_sync(0xffffffffu, dq[q], o);
-#pragma unroll
-      for (int q = 0; q < kInvGroup; ++q) {
-        const float f = tk * dq[q];
-#pragma unroll
-        for (int ri = 0; ri < NR; ++ri) yr[ri][q] = fmaf(-f, hr[ri], yr[ri][q]);
-      }
-    }
+    };
+    if (g <= 4)
+      back_transform(IntTag<4>{});
+    else
+      back_transform(IntTag<8>{});
     LRD_STAMP(6);
     // modified Gram-Schmidt in descending eigenvalue order
 #pragma unroll
