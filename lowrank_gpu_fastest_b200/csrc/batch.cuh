@@ -88,14 +88,6 @@ __global__ void __maxnreg__(64) gram_z_batch_kernel(const BatchVol* __restrict__
   gram_z_body<KS>(&V.map, V.gv, V.g, V.tab, 0, V.ring, (int)ncols, 1, V.status, (int)(blockIdx.x - off[i]));
 }
 
-// Warps per SM the single-volume eigh_reg_kernel<TMAX> reaches with the
-// registers it is built with (91 / 128 / 168 at TMAX 32 / 48 / 64): the
-// batch kernel's descriptor lookups must not lower it.
-template <int TMAX>
-__host__ __device__ constexpr int eigh_reg_min_blocks() {
-  return TMAX <= 32 ? 20 : (TMAX <= 48 ? 16 : 12);
-}
-
 template <int TMAX>
 __global__ void __launch_bounds__(32, eigh_reg_min_blocks<TMAX>()) eigh_reg_batch_kernel(const BatchVol* __restrict__ vols,
                                                             const int* __restrict__ list,

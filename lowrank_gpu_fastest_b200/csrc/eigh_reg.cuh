@@ -345,27 +345,32 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
       // j4lo enters the unrolled groups at the first live one (cases fall
       // through), so the register indices stay compile-time and the dead
       // groups cost nothing.
+      // (both own rows in one pass over the groups: each hv group is read once)
       float pr[NR];
+      float s0[NR], s1[NR], s2[NR], s3[NR];
 #pragma unroll
-      for (int ri = 0; ri < NR; ++ri) {
-        float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+      for (int ri = 0; ri < NR; ++ri) s0[ri] = s1[ri] = s2[ri] = s3[ri] = 0.f;
 #define LRD_MV(J)                                                   \
   case J:                                                           \
     if constexpr (J < TMAX / 4) {                                   \
       const float4 v4 = reinterpret_cast<const float4*>(hv)[J];     \
-      s0 = fmaf(a[ri][4 * J + 0], v4.x, s0);                        \
-      s1 = fmaf(a[ri][4 * J + 1], v4.y, s1);                        \
-      s2 = fmaf(a[ri][4 * J + 2], v4.z, s2);                        \
-      s3 = fmaf(a[ri][4 * J + 3], v4.w, s3);                        \
+      _Pragma("unroll") for (int ri = 0; ri < NR; ++ri) {           \
+        s0[ri] = fmaf(a[ri][4 * J + 0], v4.x, s0[ri]);              \
+        s1[ri] = fmaf(a[ri][4 * J + 1], v4.y, s1[ri]);              \
+        s2[ri] = fmaf(a[ri][4 * J + 2], v4.z, s2[ri]);              \
+        s3[ri] = fmaf(a[ri][4 * J + 3], v4.w, s3[ri]);              \
+      }                                                             \
     }
-        switch (j4lo) {
-          LRD_MV(0) LRD_MV(1) LRD_MV(2) LRD_MV(3) LRD_MV(4) LRD_MV(5) LRD_MV(6) LRD_MV(7)
-          LRD_MV(8) LRD_MV(9) LRD_MV(10) LRD_MV(11) LRD_MV(12) LRD_MV(13) LRD_MV(14) LRD_MV(15)
-          default: break;
-        }
+      switch (j4lo) {
+        LRD_MV(0) LRD_MV(1) LRD_MV(2) LRD_MV(3) LRD_MV(4) LRD_MV(5) LRD_MV(6) LRD_MV(7)
+        LRD_MV(8) LRD_MV(9) LRD_MV(10) LRD_MV(11) LRD_MV(12) LRD_MV(13) LRD_MV(14) LRD_MV(15)
+        default: break;
+      }
 #undef LRD_MV
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
         const int r = lane + 32 * ri;
-        pr[ri] = (r >= k + 1 && r < n) ? taui * ((s0 + s1) + (s2 + s3)) : 0.f;
+        pr[ri] = (r >= k + 1 && r < n) ? taui * ((s0[ri] + s1[ri]) + (s2[ri] + s3[ri])) : 0.f;
       }
       float part2 = 0.f;
 #pragma unroll
@@ -381,25 +386,24 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
       __syncwarp();
       // A22 -= v w^T + w v^T on own rows, columns j >= k+1 (ws, hv zero
       // below), live column groups only as above
-#pragma unroll
-      for (int ri = 0; ri < NR; ++ri) {
-#define LRD_UPD(J)                                                                   \
-  case J:                                                                            \
-    if constexpr (J < TMAX / 4) {                                                    \
-      const float4 v4 = reinterpret_cast<const float4*>(hv)[J];                      \
-      const float4 w4 = reinterpret_cast<const float4*>(ws)[J];                      \
-      a[ri][4 * J + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * J + 0])); \
-      a[ri][4 * J + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * J + 1])); \
-      a[ri][4 * J + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * J + 2])); \
-      a[ri][4 * J + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * J + 3])); \
+#define LRD_UPD(J)                                                                     \
+  case J:                                                                              \
+    if constexpr (J < TMAX / 4) {                                                      \
+      const float4 v4 = reinterpret_cast<const float4*>(hv)[J];                        \
+      const float4 w4 = reinterpret_cast<const float4*>(ws)[J];                        \
+      _Pragma("unroll") for (int ri = 0; ri < NR; ++ri) {                              \
+        a[ri][4 * J + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * J + 0])); \
+        a[ri][4 * J + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * J + 1])); \
+        a[ri][4 * J + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * J + 2])); \
+        a[ri][4 * J + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * J + 3])); \
+      }                                                                                \
     }
-        switch (j4lo) {
-          LRD_UPD(0) LRD_UPD(1) LRD_UPD(2) LRD_UPD(3) LRD_UPD(4) LRD_UPD(5) LRD_UPD(6) LRD_UPD(7)
-          LRD_UPD(8) LRD_UPD(9) LRD_UPD(10) LRD_UPD(11) LRD_UPD(12) LRD_UPD(13) LRD_UPD(14) LRD_UPD(15)
-          default: break;
-        }
-#undef LRD_UPD
+      switch (j4lo) {
+        LRD_UPD(0) LRD_UPD(1) LRD_UPD(2) LRD_UPD(3) LRD_UPD(4) LRD_UPD(5) LRD_UPD(6) LRD_UPD(7)
+        LRD_UPD(8) LRD_UPD(9) LRD_UPD(10) LRD_UPD(11) LRD_UPD(12) LRD_UPD(13) LRD_UPD(14) LRD_UPD(15)
+        default: break;
       }
+#undef LRD_UPD
     }
     __syncwarp();  // xk, ws are rewritten by the next step
   }
@@ -603,6 +607,14 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
     __syncwarp();
   }
   LRD_STAMP(7);
+}
+
+// Warps per SM the single-volume eigh_reg_kernel<TMAX> reaches with the
+// registers it is built with (91 / 128 / 168 at TMAX 32 / 48 / 64): the
+// packed batch kernel's descriptor lookups must not lower it.
+template <int TMAX>
+__host__ __device__ constexpr int eigh_reg_min_blocks() {
+  return TMAX <= 32 ? 20 : (TMAX <= 48 ? 16 : 12);
 }
 
 template <int TMAX>
