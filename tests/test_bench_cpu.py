@@ -87,3 +87,46 @@ def test_rank_mismatch_counts():
     assert r == dict(n=4, vs_step0=1, vs_fp64=2, step0_vs_fp64=1)
     assert "vs fp64" in report.rank_table([dict(case="c", shape=(4, 4, 4, 8), patch=(3, 3, 3), stride=1,
                                                 form="plain", **r)])
+
+
+def test_report_kernel_name_and_launch_table(tmp_path):
+    from lowrank_gpu_fastest_b200 import report
+
+    assert report.kernel_name("void lrd::eigh_reg_kernel<48>(const float *, float *, int)") == "eigh_reg_kernel"
+    assert report.kernel_name("lrd::(anonymous namespace)::k<lrd::Q<2>, true>(int)") == "k"
+    # an ncu launch-list CSV: preamble lines, a header, one row per launch and metric
+    rows = [
+        "==PROF== Connected to process 1",
+        '"ID","Kernel Name","Metric Name","Metric Unit","Metric Value"',
+        '"0","void lrd::gram_z_kernel<2>(CUtensorMap, float *)","gpu__time_duration.sum","usecond","600.0"',
+        '"1","void lrd::eigh_reg_kernel<48>(const float *)","gpu__time_duration.sum","usecond","1,000.0"',
+        '"2","void lrd::eigh_reg_kernel<48>(const float *)","gpu__time_duration.sum","msecond","1.0"',
+        '"3","void at::native::elementwise_kernel<128>(int)","gpu__time_duration.sum","nsecond","400000"',
+        '"4","void lrd::gram_z_kernel<2>(CUtensorMap, float *)","dram__bytes_read.sum","byte","5"',
+    ]
+    f = tmp_path / "launches.csv"
+    f.write_text("\n".join(rows) + "\n")
+    t = report.ncu_launch_table(str(f))
+    assert [r["kernel"] for r in t] == ["eigh_reg_kernel", "gram_z_kernel", "elementwise_kernel"]
+    assert t[0]["launches"] == 2 and t[0]["total_ms"] == pytest.approx(2.0)
+    assert t[1]["launches"] == 1 and t[1]["mean_us"] == pytest.approx(600.0)
+    assert sum(r["share"] for r in t) == pytest.approx(1.0)
+    assert t[0]["share"] == pytest.approx(2.0 / 3.0)
+    t2 = report.ncu_launch_table(str(f), skip="elementwise")
+    assert [r["kernel"] for r in t2] == ["eigh_reg_kernel", "gram_z_kernel"]
+    assert t2[0]["share"] == pytest.approx(2.0 / 2.6)
+
+
+def test_report_summary_table():
+    from lowrank_gpu_fastest_b200 import report
+
+    line = dict(metric="patches/s", value=4.5e6, unit="patches/s", n_gpus=1, ms_per_step=2.8,
+                config=dict(workload="96x96x48x48", form="plain"), e2e=dict(value=3.4e6),
+                roofline=dict(kernel="recon_warp_kernel", frac=0.25), clocks=dict(sm_mhz=1965))
+    ref = dict(impl="reference", value=7000.0, unit="patches/s", n_gpus=1, ms_per_step=1800.0,
+               config=dict(workload="96x96x48x48"))
+    md = report.summary([line, ref]).splitlines()
+    assert md[0].startswith("| impl | workload | form |")
+    assert len(md) == 4
+    assert "4,500,000 patches/s" in md[2] and "recon_warp_kernel 0.250" in md[2] and "1965" in md[2]
+    assert md[3].startswith("| reference | 96x96x48x48 |")
