@@ -99,7 +99,8 @@ struct lrd_plan {
   std::vector<int32_t> h_corner_x, h_brick_x;
   cudaStream_t io_in = nullptr, io_out = nullptr;
   cudaStream_t io_prep[3] = {nullptr, nullptr, nullptr};  // centre + Gram of slab s on io_prep[s % 3]
-  cudaStream_t io_recon = nullptr;                         // reconstruction of the slabs
+  cudaStream_t io_recon = nullptr;                         // reconstruction of the slabs (even ones in
+  cudaStream_t io_recon2 = nullptr;                        //   the host pipeline; odd ones on io_recon2)
   cudaStream_t io_solve = nullptr;                         // solves of odd slabs (even ones: the caller's)
   std::vector<cudaEvent_t> io_events;  // 5 per slab + 1
   // device-resident pipeline of lrd_denoise: x-slabs whose Gram, solve and
@@ -121,9 +122,13 @@ struct lrd_plan {
 namespace {
 constexpr int kProfRing = 256;
 constexpr int kIoSlabs = 16;     // event capacity of the host-buffer pipeline
-// x-slabs the host-buffer pipeline uses. Measured e2e at 96x96x48x48 / 11^3 /
-// stride 3 on B200 (ms): 4 slabs 4.73, 6 4.74, 8 4.62, 10 4.55, 12 4.62, 16 5.05.
-constexpr int kIoSlabsUsed = 10;
+// x-slabs the host-buffer pipeline uses (about 7 MiB of input each, at most
+// this many). Measured e2e at 96x96x48x48 / 11^3 / stride 3 on B200 (ms), one
+// reconstruction stream: 4 slabs 4.73, 6 4.74, 8 4.62, 10 4.55, 12 4.62, 16
+// 5.05; with the current kernels 8 3.61, 10 3.60, 12 3.62; two alternating
+// reconstruction streams: 8 3.61, 10 3.51, 12 3.48.
+constexpr int kIoSlabsUsed = 12;
+constexpr long long kIoSlabBytes = 7ll << 20;
 }
 
 namespace {
@@ -844,8 +849,21 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   {
     cudaError_t e1 = cudaStreamCreateWithFlags(&P->io_in, cudaStreamNonBlocking);
     cudaError_t e2 = cudaStreamCreateWithFlags(&P->io_out, cudaStreamNonBlocking);
-    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_recon, &P->io_solve}) {
+    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_solve}) {
       cudaError_t e4 = cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking);
+      if (e4 != cudaSuccess) {
+        *ps = nullptr;
+        if (e1 == cudaSuccess) e1 = e4;
+      }
+    }
+    // the reconstruction streams at the highest priority: a slab's bricks are
+    // reconstructed (and copied out) as soon as its solve ends, ahead of the
+    // next slabs' Grams (e2e 3.51 -> 3.50 ms at the headline; the solves at the
+    // highest priority instead measured slower)
+    int prio_lo = 0, prio_hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess) prio_hi = 0;
+    for (cudaStream_t* ps : {&P->io_recon, &P->io_recon2}) {
+      cudaError_t e4 = cudaStreamCreateWithPriority(ps, cudaStreamNonBlocking, prio_hi);
       if (e4 != cudaSuccess) {
         *ps = nullptr;
         if (e1 == cudaSuccess) e1 = e4;
@@ -972,6 +990,7 @@ int lrd_plan_destroy(lrd_plan* P) {
   for (auto ps : P->io_prep)
     if (ps) cudaStreamDestroy(ps);
   if (P->io_recon) cudaStreamDestroy(P->io_recon);
+  if (P->io_recon2) cudaStreamDestroy(P->io_recon2);
   if (P->io_solve) cudaStreamDestroy(P->io_solve);
   if (P->d_tables) cudaFree(P->d_tables);
   delete P;
@@ -1115,9 +1134,10 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   // Gram matrices on io_prep[s % 3] (a slab's Gram launch is a fraction of a
   // wave, so three slabs' Grams run side by side); solve the slab's patches,
   // refine their near-ties on the compute stream ``stream``; reconstruct the
-  // bricks whose touching patches are now all final on the reconstruction
-  // stream (overlapping the next slab's solve); copy those bricks' output
-  // planes back (copy-out stream). Events order: copy-in(s) -> centre(s)
+  // bricks whose touching patches are now all final on one of two
+  // reconstruction streams (alternating, so one slab's reconstruction fills
+  // the tail of the previous one's, and both overlap the next slab's solve);
+  // copy those bricks' output planes back (copy-out stream). Events order: copy-in(s) -> centre(s)
   // (after centre(s - 1), whose planes the slab's columns share) -> Gram(s)
   // -> solve(s) -> reconstruct(s) -> copy-out(s).
   std::lock_guard<std::mutex> lk(P->pipe_mu);  // the plan's streams and events
@@ -1139,11 +1159,12 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   LRD_CUDA(cudaStreamWaitEvent(P->io_out, start, 0));
   for (auto ps : P->io_prep) LRD_CUDA(cudaStreamWaitEvent(ps, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_recon2, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_solve, start, 0));
-  // about 8 MiB of input per slab, at most kIoSlabsUsed slabs: a small volume's
-  // slabs would be launch- and event-bound
+  // about kIoSlabBytes of input per slab, at most kIoSlabsUsed slabs: a small
+  // volume's slabs would be launch- and event-bound
   const long long vbytes = (long long)sizeof(float) * P->nvox * g.nt;
-  const int S = std::max(1, std::min<int>({kIoSlabsUsed, g.ncx, (int)((vbytes + (8ll << 20) - 1) >> 23)}));
+  const int S = std::max(1, std::min<int>({kIoSlabsUsed, g.ncx, (int)((vbytes + kIoSlabBytes - 1) / kIoSlabBytes)}));
   int planes_in = 0, ci_done = 0, bx_done = 0;
   const long long colz = (long long)g.ncy, patz = (long long)g.ncy * g.ncz, brz = (long long)g.nby * g.nbz;
   for (int s = 0; s < S; ++s) {
@@ -1174,9 +1195,15 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
     int bx_end = bx_done;
     while (bx_end < g.nbx && (lastslab || P->h_brick_x[2 * bx_end + 1] < ci_end)) ++bx_end;
     LRD_CUDA(cudaEventRecord(ev(s, 4), solve));
-    LRD_CUDA(cudaStreamWaitEvent(P->io_recon, ev(s, 4), 0));
-    if ((rc = run_recon(P, ws, d_out, P->io_recon, bx_done * brz, bx_end * brz))) return rc;
-    LRD_CUDA(cudaEventRecord(ev(s, 3), P->io_recon));
+    // slab s's bricks touch patches of slab s, s - 1 and possibly earlier
+    // slabs (a brick's patches span four corners): s and s - 1 are waited for
+    // here, the earlier ones through the previous reconstruction on the same
+    // stream (slab s - 2's, which waited for s - 2 and s - 3)
+    cudaStream_t recon = (s & 1) ? P->io_recon2 : P->io_recon;
+    LRD_CUDA(cudaStreamWaitEvent(recon, ev(s, 4), 0));
+    if (s > 0) LRD_CUDA(cudaStreamWaitEvent(recon, ev(s - 1, 4), 0));
+    if ((rc = run_recon(P, ws, d_out, recon, bx_done * brz, bx_end * brz))) return rc;
+    LRD_CUDA(cudaEventRecord(ev(s, 3), recon));
     if (bx_end > bx_done) {
       const long long x0 = (long long)bx_done * g.bx, x1 = std::min<long long>((long long)bx_end * g.bx, g.nx);
       LRD_CUDA(cudaStreamWaitEvent(P->io_out, ev(s, 3), 0));
@@ -1185,7 +1212,10 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
     }
     bx_done = bx_end;
   }
-  LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 1, 3), 0));  // the last reconstruction joins the caller's stream
+  // the last two reconstructions join the caller's stream (each followed
+  // every solve before it)
+  LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 1, 3), 0));
+  if (S >= 2) LRD_CUDA(cudaStreamWaitEvent(st, ev(S - 2, 3), 0));
   if (d_ranks) LRD_CUDA(cudaMemcpyAsync(d_ranks, rank, sizeof(int32_t) * g.npatch, cudaMemcpyDeviceToDevice, st));
   if (h_ranks) {
     LRD_CUDA(cudaEventRecord(ev(S - 1, 4), st));
