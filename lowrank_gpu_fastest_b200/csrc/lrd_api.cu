@@ -101,7 +101,8 @@ struct lrd_plan {
   cudaStream_t io_prep[3] = {nullptr, nullptr, nullptr};  // centre + Gram of slab s on io_prep[s % 3]
   cudaStream_t io_recon = nullptr;                         // reconstruction of the slabs (even ones in
   cudaStream_t io_recon2 = nullptr;                        //   the host pipeline; odd ones on io_recon2)
-  cudaStream_t io_solve = nullptr;                         // solves of odd slabs (even ones: the caller's)
+  cudaStream_t io_solve = nullptr;                         // solves of odd slabs (even ones: the caller's;
+  cudaStream_t io_solve2 = nullptr;                        //   host pipeline: slab s on s % 3 of the three)
   std::vector<cudaEvent_t> io_events;  // 5 per slab + 1
   // device-resident pipeline of lrd_denoise: x-slabs whose Gram, solve and
   // reconstruction overlap on the plan's streams (1 = one pass per phase);
@@ -122,13 +123,16 @@ struct lrd_plan {
 namespace {
 constexpr int kProfRing = 256;
 constexpr int kIoSlabs = 16;     // event capacity of the host-buffer pipeline
-// x-slabs the host-buffer pipeline uses (about 7 MiB of input each, at most
+// x-slabs the host-buffer pipeline uses (about 3.5 MiB of input each, at most
 // this many). Measured e2e at 96x96x48x48 / 11^3 / stride 3 on B200 (ms), one
 // reconstruction stream: 4 slabs 4.73, 6 4.74, 8 4.62, 10 4.55, 12 4.62, 16
 // 5.05; with the current kernels 8 3.61, 10 3.60, 12 3.62; two alternating
-// reconstruction streams: 8 3.61, 10 3.51, 12 3.48.
-constexpr int kIoSlabsUsed = 12;
-constexpr long long kIoSlabBytes = 7ll << 20;
+// reconstruction streams: 8 3.61, 10 3.51, 12 3.48; and two / three / four
+// solve streams: 12 slabs 3.48 / 3.48 / 3.60, 16 3.49 / 3.38 / 3.53, 20
+// 3.63 / 3.45 / 3.65, 24 3.90 / 3.60 / 3.73. At 48x48x24x48 (10 MiB), three
+// solve streams: 1 slab 0.83, 2 0.73, 3 0.70, 4 0.72, 5 0.73.
+constexpr int kIoSlabsUsed = 16;
+constexpr long long kIoSlabBytes = 7ll << 19;
 }
 
 namespace {
@@ -849,7 +853,7 @@ int create_plan(const lrd_problem* pr, const std::vector<int32_t>* x_corners, lr
   {
     cudaError_t e1 = cudaStreamCreateWithFlags(&P->io_in, cudaStreamNonBlocking);
     cudaError_t e2 = cudaStreamCreateWithFlags(&P->io_out, cudaStreamNonBlocking);
-    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_solve}) {
+    for (cudaStream_t* ps : {&P->io_prep[0], &P->io_prep[1], &P->io_prep[2], &P->io_solve, &P->io_solve2}) {
       cudaError_t e4 = cudaStreamCreateWithFlags(ps, cudaStreamNonBlocking);
       if (e4 != cudaSuccess) {
         *ps = nullptr;
@@ -992,6 +996,7 @@ int lrd_plan_destroy(lrd_plan* P) {
   if (P->io_recon) cudaStreamDestroy(P->io_recon);
   if (P->io_recon2) cudaStreamDestroy(P->io_recon2);
   if (P->io_solve) cudaStreamDestroy(P->io_solve);
+  if (P->io_solve2) cudaStreamDestroy(P->io_solve2);
   if (P->d_tables) cudaFree(P->d_tables);
   delete P;
   return LRD_OK;
@@ -1161,6 +1166,7 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   LRD_CUDA(cudaStreamWaitEvent(P->io_recon, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_recon2, start, 0));
   LRD_CUDA(cudaStreamWaitEvent(P->io_solve, start, 0));
+  LRD_CUDA(cudaStreamWaitEvent(P->io_solve2, start, 0));
   // about kIoSlabBytes of input per slab, at most kIoSlabsUsed slabs: a small
   // volume's slabs would be launch- and event-bound
   const long long vbytes = (long long)sizeof(float) * P->nvox * g.nt;
@@ -1185,9 +1191,10 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
     planes_in = std::max(planes_in, x_need);
     if ((rc = run_gram(P, ws, gv, prep, ci_done * colz, ci_end * colz, s == 0))) return rc;
     LRD_CUDA(cudaEventRecord(ev(s, 2), prep));
-    // successive slabs' solves on two streams, each slab with its own near-tie
-    // queue: a slab's solve takes a matrix's latency however few it holds
-    cudaStream_t solve = (s & 1) ? P->io_solve : st;
+    // successive slabs' solves on three streams, each slab with its own
+    // near-tie queue: a slab's solve takes a matrix's latency however few it
+    // holds, so up to three run side by side
+    cudaStream_t solve = (s % 3 == 0) ? st : (s % 3 == 1 ? P->io_solve : P->io_solve2);
     LRD_CUDA(cudaStreamWaitEvent(solve, ev(s, 2), 0));
     if ((rc = run_eigh(P, ws, gv, gv, nullptr, rank, wgt, solve, ci_done * patz, ci_end * patz, false, d_in, s)))
       return rc;
