@@ -1137,14 +1137,16 @@ int lrd_denoise_host(const lrd_plan* P, const float* h_vol, float* h_out, int32_
   // Pipeline over x-slabs of patch corners. Slab s: copy in the x-planes its
   // patch columns need (copy-in stream); centre them and form those columns'
   // Gram matrices on io_prep[s % 3] (a slab's Gram launch is a fraction of a
-  // wave, so three slabs' Grams run side by side); solve the slab's patches,
-  // refine their near-ties on the compute stream ``stream``; reconstruct the
-  // bricks whose touching patches are now all final on one of two
-  // reconstruction streams (alternating, so one slab's reconstruction fills
-  // the tail of the previous one's, and both overlap the next slab's solve);
-  // copy those bricks' output planes back (copy-out stream). Events order: copy-in(s) -> centre(s)
-  // (after centre(s - 1), whose planes the slab's columns share) -> Gram(s)
-  // -> solve(s) -> reconstruct(s) -> copy-out(s).
+  // wave, so three slabs' Grams run side by side); solve the slab's patches
+  // and refine their near-ties on one of three solve streams (the caller's
+  // ``stream``, io_solve, io_solve2: s % 3); reconstruct the bricks whose
+  // touching patches are now all final on one of two reconstruction streams
+  // (alternating, so one slab's reconstruction fills the tail of the
+  // previous one's, and both overlap the next slabs' solves); copy those
+  // bricks' output planes back (copy-out stream). Events order: copy-in(s)
+  // -> centre(s) (after centre(s - 1), whose planes the slab's columns
+  // share) -> Gram(s) -> solve(s) -> reconstruct(s) (also after solve(s - 1))
+  // -> copy-out(s).
   std::lock_guard<std::mutex> lk(P->pipe_mu);  // the plan's streams and events
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   char* ws = static_cast<char*>(d_ws);
