@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(32, eigh_reg_min_blocks<TMAX>()) eigh_reg_batc
                                                             const long long* __restrict__ off, int n) {
   const int i = batch_find(off, n, blockIdx.x);
   const BatchVol& V = vols[list[i]];
-  eigh_reg_body<TMAX>(V.gv, V.gv, nullptr, V.rank, V.wgt, V.sig2, V.g.nt, V.g.nvox_patch, 0, V.refine,
+  eigh_reg_body<TMAX, false>(V.gv, V.gv, nullptr, V.rank, V.wgt, V.sig2, V.g.nt, V.g.nvox_patch, 0, V.refine,
                       V.refine + 64, (long long)blockIdx.x - off[i]);
 }
 

@@ -234,9 +234,173 @@ __device__ __forceinline__ void bisect_reg(const float* d, const float* e, const
   tnorm_out = tnorm;
 }
 
+// For TMAX in (32, 48] the rows 32..TMAX-1 are held as half-rows: lane l
+// holds row l whole and, of row 32 + (l & 15), the columns 4J + 2h and
+// 4J + 2h + 1 of every 4-column group J (h = l >> 4), so 1.5 rows of
+// registers per lane instead of 2 (72 instead of 96 at TMAX 48: more warps
+// per SM). Every FMA chain of the two-row layout stays in one lane in the
+// same order - the matvec's column-residue accumulators s0, s1 (h = 0) and
+// s2, s3 (h = 1), each element's rank-2 update - and the half-row sum is
+// (s0 + s1) + (s2 + s3) after one exchange, so the reduction is
+// bit-identical to the two-row layout's.
+template <int TMAX>
+__host__ __device__ constexpr bool eigh_reg_half() {
+  return TMAX > 32 && TMAX <= 48 && TMAX % 4 == 0;
+}
+
+// Load (exact power-of-two scaling) and Householder tridiagonalisation in the
+// half-row layout: d, e, tau and the packed reflector rows HV as the two-row
+// code writes them; returns the unscaling factor and the end of the packed
+// rows. xk and ws are the row-broadcast and w vectors (TMAX floats each).
+template <int TMAX>
+__device__ __forceinline__ void tridiag_half(const float* G, int n, float* HV, float* d, float* e, float* tau,
+                                             float* xk, float* ws, float& unscale_out, int& hbase_out) {
+  constexpr int NG = TMAX / 4;  // 4-column groups
+  const int lane = threadIdx.x & 31;
+  const int h = lane >> 4;
+  const int r1 = 32 + (lane & 15);
+  const bool v0 = lane < n, v1 = r1 < n;
+  float a0[TMAX], a1[TMAX / 2];
+  float dmax = 0.f;
+#pragma unroll
+  for (int j = 0; j < TMAX; ++j) a0[j] = (v0 && j < n) ? G[(long long)lane * n + j] : 0.f;
+#pragma unroll
+  for (int J = 0; J < NG; ++J)
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int c = 4 * J + 2 * h + t;
+      a1[2 * J + t] = (v1 && c < n) ? G[(long long)r1 * n + c] : 0.f;
+    }
+  if (v0) dmax = fmaxf(dmax, fabsf(G[(long long)lane * n + lane]));
+  if (v1) dmax = fmaxf(dmax, fabsf(G[(long long)r1 * n + r1]));
+  dmax = warp_max(dmax);
+  int ex = 0;
+  if (dmax > 0.f && isfinite(dmax)) frexpf(dmax, &ex);
+  const float scale = ldexpf(1.f, -ex);
+  unscale_out = ldexpf(1.f, ex);
+#pragma unroll
+  for (int j = 0; j < TMAX; ++j) a0[j] *= scale;
+#pragma unroll
+  for (int j = 0; j < TMAX / 2; ++j) a1[j] *= scale;
+
+  LRD_STAMP(1);
+  int hbase = 0;  // packed offset of row k of HV
+  for (int k = 0; k < n; ++k) {
+    // row k (= column k) into xk: a whole row from its lane, a half-row from
+    // its two lanes
+    if (k < 32) {
+      if (lane == k) {
+#pragma unroll
+        for (int J = 0; J < NG; ++J)
+          reinterpret_cast<float4*>(xk)[J] = make_float4(a0[4 * J], a0[4 * J + 1], a0[4 * J + 2], a0[4 * J + 3]);
+      }
+    } else if ((lane & 15) == k - 32) {
+#pragma unroll
+      for (int J = 0; J < NG; ++J)
+        *reinterpret_cast<float2*>(xk + 4 * J + 2 * h) = make_float2(a1[2 * J], a1[2 * J + 1]);
+    }
+    __syncwarp();
+    if (k >= n - 2) {
+      if (lane == 0) {
+        d[k] = xk[k];
+        e[k] = (k == n - 2) ? xk[k + 1] : 0.f;
+        tau[k] = 0.f;
+      }
+      __syncwarp();
+      continue;
+    }
+    const float xr0 = v0 ? xk[lane] : 0.f;
+    const float xr1 = v1 ? xk[r1] : 0.f;
+    float part = 0.f;
+    if (lane >= k + 2 && lane < n) part = fmaf(xr0, xr0, part);
+    if (h == 0 && r1 >= k + 2 && r1 < n) part = fmaf(xr1, xr1, part);
+    const float xnorm2 = warp_sum(part);
+    const float alpha = xk[k + 1];
+    float taui = 0.f, beta = alpha, sc = 0.f;
+    if (xnorm2 > 0.f) {
+      beta = -copysignf(sqrtf(fmaf(alpha, alpha, xnorm2)), alpha);
+      taui = (beta - alpha) / beta;
+      sc = 1.f / (alpha - beta);
+    }
+    if (lane == 0) {
+      d[k] = xk[k];
+      e[k] = beta;
+      tau[k] = taui;
+    }
+    const int j4lo = (k + 1) >> 2;
+    float* hv = HV + hbase - 4 * j4lo;
+    hbase += TMAX - 4 * j4lo;
+    const float vr0 = (lane == k + 1) ? 1.f : ((lane >= k + 2 && lane < n) ? xr0 * sc : 0.f);
+    const float vr1 = (r1 == k + 1) ? 1.f : ((r1 >= k + 2 && r1 < n) ? xr1 * sc : 0.f);
+    if (lane >= 4 * j4lo && lane < TMAX) hv[lane] = vr0;
+    if (h == 0 && r1 >= 4 * j4lo && r1 < TMAX) hv[r1] = vr1;
+    __syncwarp();
+    if (taui != 0.f) {
+      // p = taui * A22 v (live column groups from j4lo, as in the two-row code)
+      const float4* hv4 = reinterpret_cast<const float4*>(hv);
+      float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, t0 = 0.f, t1 = 0.f;
+#define LRD_MVH(J)                                        \
+  case J:                                                 \
+    if constexpr (J < NG) {                               \
+      const float4 v4 = hv4[J];                           \
+      s0 = fmaf(a0[4 * J + 0], v4.x, s0);                 \
+      s1 = fmaf(a0[4 * J + 1], v4.y, s1);                 \
+      s2 = fmaf(a0[4 * J + 2], v4.z, s2);                 \
+      s3 = fmaf(a0[4 * J + 3], v4.w, s3);                 \
+      t0 = fmaf(a1[2 * J + 0], h ? v4.z : v4.x, t0);      \
+      t1 = fmaf(a1[2 * J + 1], h ? v4.w : v4.y, t1);      \
+    }
+      switch (j4lo) {
+        LRD_MVH(0) LRD_MVH(1) LRD_MVH(2) LRD_MVH(3) LRD_MVH(4) LRD_MVH(5)
+        LRD_MVH(6) LRD_MVH(7) LRD_MVH(8) LRD_MVH(9) LRD_MVH(10) LRD_MVH(11)
+        default: break;
+      }
+#undef LRD_MVH
+      const float pr0 = (lane >= k + 1 && lane < n) ? taui * ((s0 + s1) + (s2 + s3)) : 0.f;
+      const float pair = t0 + t1;  // s0 + s1 (h = 0) or s2 + s3 (h = 1) of the half-row
+      const float other = __shfl_xor_sync(0xffffffffu, pair, 16);
+      const float pr1 = (r1 >= k + 1 && r1 < n) ? taui * (h ? other + pair : pair + other) : 0.f;
+      float part2 = 0.f;
+      part2 = fmaf(pr0, vr0, part2);
+      part2 = fmaf(h ? 0.f : pr1, h ? 0.f : vr1, part2);  // the half-row counted once
+      const float kc = -0.5f * taui * warp_sum(part2);
+      const float wr0 = fmaf(kc, vr0, pr0);
+      const float wr1 = fmaf(kc, vr1, pr1);
+      if (lane < TMAX) ws[lane] = wr0;
+      if (h == 0 && r1 < TMAX) ws[r1] = wr1;
+      __syncwarp();
+      // A22 -= v w^T + w v^T (live column groups)
+      const float4* ws4 = reinterpret_cast<const float4*>(ws);
+#define LRD_UPDH(J)                                                                   \
+  case J:                                                                             \
+    if constexpr (J < NG) {                                                           \
+      const float4 v4 = hv4[J];                                                       \
+      const float4 w4 = ws4[J];                                                       \
+      a0[4 * J + 0] = fmaf(-vr0, w4.x, fmaf(-wr0, v4.x, a0[4 * J + 0]));              \
+      a0[4 * J + 1] = fmaf(-vr0, w4.y, fmaf(-wr0, v4.y, a0[4 * J + 1]));              \
+      a0[4 * J + 2] = fmaf(-vr0, w4.z, fmaf(-wr0, v4.z, a0[4 * J + 2]));              \
+      a0[4 * J + 3] = fmaf(-vr0, w4.w, fmaf(-wr0, v4.w, a0[4 * J + 3]));              \
+      const float va = h ? v4.z : v4.x, vb = h ? v4.w : v4.y;                         \
+      const float wa = h ? w4.z : w4.x, wb = h ? w4.w : w4.y;                         \
+      a1[2 * J + 0] = fmaf(-vr1, wa, fmaf(-wr1, va, a1[2 * J + 0]));                  \
+      a1[2 * J + 1] = fmaf(-vr1, wb, fmaf(-wr1, vb, a1[2 * J + 1]));                  \
+    }
+      switch (j4lo) {
+        LRD_UPDH(0) LRD_UPDH(1) LRD_UPDH(2) LRD_UPDH(3) LRD_UPDH(4) LRD_UPDH(5)
+        LRD_UPDH(6) LRD_UPDH(7) LRD_UPDH(8) LRD_UPDH(9) LRD_UPDH(10) LRD_UPDH(11)
+        default: break;
+      }
+#undef LRD_UPDH
+    }
+    __syncwarp();  // xk, ws are rewritten by the next step
+  }
+  hbase_out = hbase;
+}
+
 // Body of one warp's matrix ``b`` (the launch's patch index; the patch is
 // patch0 + b), shared by the single-volume kernel and the packed launch.
-template <int TMAX>
+// HALF: the half-row tridiagonalisation (TMAX in (32, 48]; same results).
+template <int TMAX, bool HALF = eigh_reg_half<TMAX>()>
 __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, float* __restrict__ lam_out,
                                               int32_t* __restrict__ ranks, float* __restrict__ wgt,
                                               float* __restrict__ sig2, int n, int nvox, long long patch0,
@@ -258,154 +422,162 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
   const float* G = gram + b * (long long)n * n;
   LRD_STAMP(0);
 
-  // ---- load own rows, exact power-of-two scaling -----------------------------
-  float a[NR][TMAX];
-  float dmax = 0.f;
+  // ---- load own rows (exact power-of-two scaling), Householder ---------------
+  float unscale;
+  int hbase;
+  if constexpr (HALF) {
+    tridiag_half<TMAX>(G, n, HV, d, e, tau, xk, ws, unscale, hbase);
+  } else {
+    // ---- load own rows, exact power-of-two scaling -----------------------------
+    float a[NR][TMAX];
+    float dmax = 0.f;
 #pragma unroll
-  for (int ri = 0; ri < NR; ++ri) {
-    const int r = lane + 32 * ri;
-    const bool rv = r < n;
+    for (int ri = 0; ri < NR; ++ri) {
+      const int r = lane + 32 * ri;
+      const bool rv = r < n;
 #pragma unroll
-    for (int j = 0; j < TMAX; ++j) a[ri][j] = (rv && j < n) ? G[(long long)r * n + j] : 0.f;
-    if (rv) dmax = fmaxf(dmax, fabsf(G[(long long)r * n + r]));
-  }
-  dmax = warp_max(dmax);
-  int ex = 0;
-  if (dmax > 0.f && isfinite(dmax)) frexpf(dmax, &ex);
-  const float scale = ldexpf(1.f, -ex), unscale = ldexpf(1.f, ex);
-#pragma unroll
-  for (int ri = 0; ri < NR; ++ri)
-#pragma unroll
-    for (int j = 0; j < TMAX; ++j) a[ri][j] *= scale;
-
-  LRD_STAMP(1);
-  // ---- Householder tridiagonalisation ---------------------------------------
-  int hbase = 0;  // packed offset of row k of HV
-  for (int k = 0; k < n; ++k) {
-    // owner of row k broadcasts it (= column k by symmetry)
-    if (lane == (k & 31)) {
-      if (NR == 1 || k < 32) {
-#pragma unroll
-        for (int j4 = 0; j4 < TMAX / 4; ++j4)
-          reinterpret_cast<float4*>(xk)[j4] = make_float4(a[0][4 * j4], a[0][4 * j4 + 1], a[0][4 * j4 + 2],
-                                                          a[0][4 * j4 + 3]);
-      } else {
-#pragma unroll
-        for (int j4 = 0; j4 < TMAX / 4; ++j4)
-          reinterpret_cast<float4*>(xk)[j4] = make_float4(a[NR - 1][4 * j4], a[NR - 1][4 * j4 + 1],
-                                                          a[NR - 1][4 * j4 + 2], a[NR - 1][4 * j4 + 3]);
-      }
+      for (int j = 0; j < TMAX; ++j) a[ri][j] = (rv && j < n) ? G[(long long)r * n + j] : 0.f;
+      if (rv) dmax = fmaxf(dmax, fabsf(G[(long long)r * n + r]));
     }
-    __syncwarp();
-    if (k >= n - 2) {
+    dmax = warp_max(dmax);
+    int ex = 0;
+    if (dmax > 0.f && isfinite(dmax)) frexpf(dmax, &ex);
+    const float scale = ldexpf(1.f, -ex);
+    unscale = ldexpf(1.f, ex);
+#pragma unroll
+    for (int ri = 0; ri < NR; ++ri)
+#pragma unroll
+      for (int j = 0; j < TMAX; ++j) a[ri][j] *= scale;
+
+    LRD_STAMP(1);
+    // ---- Householder tridiagonalisation ---------------------------------------
+    hbase = 0;  // packed offset of row k of HV
+    for (int k = 0; k < n; ++k) {
+      // owner of row k broadcasts it (= column k by symmetry)
+      if (lane == (k & 31)) {
+        if (NR == 1 || k < 32) {
+#pragma unroll
+          for (int j4 = 0; j4 < TMAX / 4; ++j4)
+            reinterpret_cast<float4*>(xk)[j4] = make_float4(a[0][4 * j4], a[0][4 * j4 + 1], a[0][4 * j4 + 2],
+                                                            a[0][4 * j4 + 3]);
+        } else {
+#pragma unroll
+          for (int j4 = 0; j4 < TMAX / 4; ++j4)
+            reinterpret_cast<float4*>(xk)[j4] = make_float4(a[NR - 1][4 * j4], a[NR - 1][4 * j4 + 1],
+                                                            a[NR - 1][4 * j4 + 2], a[NR - 1][4 * j4 + 3]);
+        }
+      }
+      __syncwarp();
+      if (k >= n - 2) {
+        if (lane == 0) {
+          d[k] = xk[k];
+          e[k] = (k == n - 2) ? xk[k + 1] : 0.f;
+          tau[k] = 0.f;
+        }
+        __syncwarp();
+        continue;
+      }
+      float xr[NR];
+      float part = 0.f;
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
+        const int r = lane + 32 * ri;
+        xr[ri] = (r < n) ? xk[r] : 0.f;
+        if (r >= k + 2 && r < n) part = fmaf(xr[ri], xr[ri], part);
+      }
+      const float xnorm2 = warp_sum(part);
+      const float alpha = xk[k + 1];
+      float taui = 0.f, beta = alpha, sc = 0.f;
+      if (xnorm2 > 0.f) {
+        beta = -copysignf(sqrtf(fmaf(alpha, alpha, xnorm2)), alpha);
+        taui = (beta - alpha) / beta;
+        sc = 1.f / (alpha - beta);
+      }
       if (lane == 0) {
         d[k] = xk[k];
-        e[k] = (k == n - 2) ? xk[k + 1] : 0.f;
-        tau[k] = 0.f;
+        e[k] = beta;
+        tau[k] = taui;
+      }
+      // row k from its first live column group j4lo on; hv[c] = column c
+      const int j4lo = (k + 1) >> 2;
+      float* hv = HV + hbase - 4 * j4lo;
+      hbase += TMAX - 4 * j4lo;
+      float vr[NR];
+#pragma unroll
+      for (int ri = 0; ri < NR; ++ri) {
+        const int r = lane + 32 * ri;
+        vr[ri] = (r == k + 1) ? 1.f : ((r >= k + 2 && r < n) ? xr[ri] * sc : 0.f);
+        if (r >= 4 * j4lo && r < TMAX) hv[r] = vr[ri];
       }
       __syncwarp();
-      continue;
-    }
-    float xr[NR];
-    float part = 0.f;
+      if (taui != 0.f) {
+        // p = taui * A22 v over own rows (columns j >= k+1; hv is 0 below).
+        // The column groups j4 < j4lo are dead (and not stored): a switch on
+        // j4lo enters the unrolled groups at the first live one (cases fall
+        // through), so the register indices stay compile-time and the dead
+        // groups cost nothing.
+        // (both own rows in one pass over the groups: each hv group is read once)
+        float pr[NR];
+        float s0[NR], s1[NR], s2[NR], s3[NR];
 #pragma unroll
-    for (int ri = 0; ri < NR; ++ri) {
-      const int r = lane + 32 * ri;
-      xr[ri] = (r < n) ? xk[r] : 0.f;
-      if (r >= k + 2 && r < n) part = fmaf(xr[ri], xr[ri], part);
-    }
-    const float xnorm2 = warp_sum(part);
-    const float alpha = xk[k + 1];
-    float taui = 0.f, beta = alpha, sc = 0.f;
-    if (xnorm2 > 0.f) {
-      beta = -copysignf(sqrtf(fmaf(alpha, alpha, xnorm2)), alpha);
-      taui = (beta - alpha) / beta;
-      sc = 1.f / (alpha - beta);
-    }
-    if (lane == 0) {
-      d[k] = xk[k];
-      e[k] = beta;
-      tau[k] = taui;
-    }
-    // row k from its first live column group j4lo on; hv[c] = column c
-    const int j4lo = (k + 1) >> 2;
-    float* hv = HV + hbase - 4 * j4lo;
-    hbase += TMAX - 4 * j4lo;
-    float vr[NR];
-#pragma unroll
-    for (int ri = 0; ri < NR; ++ri) {
-      const int r = lane + 32 * ri;
-      vr[ri] = (r == k + 1) ? 1.f : ((r >= k + 2 && r < n) ? xr[ri] * sc : 0.f);
-      if (r >= 4 * j4lo && r < TMAX) hv[r] = vr[ri];
-    }
-    __syncwarp();
-    if (taui != 0.f) {
-      // p = taui * A22 v over own rows (columns j >= k+1; hv is 0 below).
-      // The column groups j4 < j4lo are dead (and not stored): a switch on
-      // j4lo enters the unrolled groups at the first live one (cases fall
-      // through), so the register indices stay compile-time and the dead
-      // groups cost nothing.
-      // (both own rows in one pass over the groups: each hv group is read once)
-      float pr[NR];
-      float s0[NR], s1[NR], s2[NR], s3[NR];
-#pragma unroll
-      for (int ri = 0; ri < NR; ++ri) s0[ri] = s1[ri] = s2[ri] = s3[ri] = 0.f;
+        for (int ri = 0; ri < NR; ++ri) s0[ri] = s1[ri] = s2[ri] = s3[ri] = 0.f;
 #define LRD_MV(J)                                                   \
-  case J:                                                           \
-    if constexpr (J < TMAX / 4) {                                   \
-      const float4 v4 = reinterpret_cast<const float4*>(hv)[J];     \
-      _Pragma("unroll") for (int ri = 0; ri < NR; ++ri) {           \
-        s0[ri] = fmaf(a[ri][4 * J + 0], v4.x, s0[ri]);              \
-        s1[ri] = fmaf(a[ri][4 * J + 1], v4.y, s1[ri]);              \
-        s2[ri] = fmaf(a[ri][4 * J + 2], v4.z, s2[ri]);              \
-        s3[ri] = fmaf(a[ri][4 * J + 3], v4.w, s3[ri]);              \
-      }                                                             \
-    }
-      switch (j4lo) {
-        LRD_MV(0) LRD_MV(1) LRD_MV(2) LRD_MV(3) LRD_MV(4) LRD_MV(5) LRD_MV(6) LRD_MV(7)
-        LRD_MV(8) LRD_MV(9) LRD_MV(10) LRD_MV(11) LRD_MV(12) LRD_MV(13) LRD_MV(14) LRD_MV(15)
-        default: break;
+    case J:                                                           \
+      if constexpr (J < TMAX / 4) {                                   \
+        const float4 v4 = reinterpret_cast<const float4*>(hv)[J];     \
+        _Pragma("unroll") for (int ri = 0; ri < NR; ++ri) {           \
+          s0[ri] = fmaf(a[ri][4 * J + 0], v4.x, s0[ri]);              \
+          s1[ri] = fmaf(a[ri][4 * J + 1], v4.y, s1[ri]);              \
+          s2[ri] = fmaf(a[ri][4 * J + 2], v4.z, s2[ri]);              \
+          s3[ri] = fmaf(a[ri][4 * J + 3], v4.w, s3[ri]);              \
+        }                                                             \
       }
+        switch (j4lo) {
+          LRD_MV(0) LRD_MV(1) LRD_MV(2) LRD_MV(3) LRD_MV(4) LRD_MV(5) LRD_MV(6) LRD_MV(7)
+          LRD_MV(8) LRD_MV(9) LRD_MV(10) LRD_MV(11) LRD_MV(12) LRD_MV(13) LRD_MV(14) LRD_MV(15)
+          default: break;
+        }
 #undef LRD_MV
 #pragma unroll
-      for (int ri = 0; ri < NR; ++ri) {
-        const int r = lane + 32 * ri;
-        pr[ri] = (r >= k + 1 && r < n) ? taui * ((s0[ri] + s1[ri]) + (s2[ri] + s3[ri])) : 0.f;
-      }
-      float part2 = 0.f;
+        for (int ri = 0; ri < NR; ++ri) {
+          const int r = lane + 32 * ri;
+          pr[ri] = (r >= k + 1 && r < n) ? taui * ((s0[ri] + s1[ri]) + (s2[ri] + s3[ri])) : 0.f;
+        }
+        float part2 = 0.f;
 #pragma unroll
-      for (int ri = 0; ri < NR; ++ri) part2 = fmaf(pr[ri], vr[ri], part2);
-      const float kc = -0.5f * taui * warp_sum(part2);
-      float wr[NR];
+        for (int ri = 0; ri < NR; ++ri) part2 = fmaf(pr[ri], vr[ri], part2);
+        const float kc = -0.5f * taui * warp_sum(part2);
+        float wr[NR];
 #pragma unroll
-      for (int ri = 0; ri < NR; ++ri) {
-        const int r = lane + 32 * ri;
-        wr[ri] = fmaf(kc, vr[ri], pr[ri]);
-        if (r < TMAX) ws[r] = wr[ri];
-      }
-      __syncwarp();
-      // A22 -= v w^T + w v^T on own rows, columns j >= k+1 (ws, hv zero
-      // below), live column groups only as above
+        for (int ri = 0; ri < NR; ++ri) {
+          const int r = lane + 32 * ri;
+          wr[ri] = fmaf(kc, vr[ri], pr[ri]);
+          if (r < TMAX) ws[r] = wr[ri];
+        }
+        __syncwarp();
+        // A22 -= v w^T + w v^T on own rows, columns j >= k+1 (ws, hv zero
+        // below), live column groups only as above
 #define LRD_UPD(J)                                                                     \
-  case J:                                                                              \
-    if constexpr (J < TMAX / 4) {                                                      \
-      const float4 v4 = reinterpret_cast<const float4*>(hv)[J];                        \
-      const float4 w4 = reinterpret_cast<const float4*>(ws)[J];                        \
-      _Pragma("unroll") for (int ri = 0; ri < NR; ++ri) {                              \
-        a[ri][4 * J + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * J + 0])); \
-        a[ri][4 * J + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * J + 1])); \
-        a[ri][4 * J + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * J + 2])); \
-        a[ri][4 * J + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * J + 3])); \
-      }                                                                                \
-    }
-      switch (j4lo) {
-        LRD_UPD(0) LRD_UPD(1) LRD_UPD(2) LRD_UPD(3) LRD_UPD(4) LRD_UPD(5) LRD_UPD(6) LRD_UPD(7)
-        LRD_UPD(8) LRD_UPD(9) LRD_UPD(10) LRD_UPD(11) LRD_UPD(12) LRD_UPD(13) LRD_UPD(14) LRD_UPD(15)
-        default: break;
+    case J:                                                                              \
+      if constexpr (J < TMAX / 4) {                                                      \
+        const float4 v4 = reinterpret_cast<const float4*>(hv)[J];                        \
+        const float4 w4 = reinterpret_cast<const float4*>(ws)[J];                        \
+        _Pragma("unroll") for (int ri = 0; ri < NR; ++ri) {                              \
+          a[ri][4 * J + 0] = fmaf(-vr[ri], w4.x, fmaf(-wr[ri], v4.x, a[ri][4 * J + 0])); \
+          a[ri][4 * J + 1] = fmaf(-vr[ri], w4.y, fmaf(-wr[ri], v4.y, a[ri][4 * J + 1])); \
+          a[ri][4 * J + 2] = fmaf(-vr[ri], w4.z, fmaf(-wr[ri], v4.z, a[ri][4 * J + 2])); \
+          a[ri][4 * J + 3] = fmaf(-vr[ri], w4.w, fmaf(-wr[ri], v4.w, a[ri][4 * J + 3])); \
+        }                                                                                \
       }
+        switch (j4lo) {
+          LRD_UPD(0) LRD_UPD(1) LRD_UPD(2) LRD_UPD(3) LRD_UPD(4) LRD_UPD(5) LRD_UPD(6) LRD_UPD(7)
+          LRD_UPD(8) LRD_UPD(9) LRD_UPD(10) LRD_UPD(11) LRD_UPD(12) LRD_UPD(13) LRD_UPD(14) LRD_UPD(15)
+          default: break;
+        }
 #undef LRD_UPD
+      }
+      __syncwarp();  // xk, ws are rewritten by the next step
     }
-    __syncwarp();  // xk, ws are rewritten by the next step
   }
   for (int i = lane; i < n; i += 32) e2[i] = (i < n - 1) ? e[i] * e[i] : 0.f;
   __syncwarp();
@@ -610,15 +782,20 @@ __device__ __forceinline__ void eigh_reg_body(const float* gram, float* vecs, fl
 }
 
 // Warps per SM the single-volume eigh_reg_kernel<TMAX> reaches with the
-// registers it is built with (91 / 128 / 168 at TMAX 32 / 48 / 64): the
+// registers it is built with (94 / 128 / 168 at TMAX 32 / 48 / 64): the
 // packed batch kernel's descriptor lookups must not lower it.
 template <int TMAX>
 __host__ __device__ constexpr int eigh_reg_min_blocks() {
   return TMAX <= 32 ? 20 : (TMAX <= 48 ? 16 : 12);
 }
 
+// At TMAX 48 the half-row tridiagonalisation measured 0.908 -> 0.885 ms on
+// the 12600 headline Grams (bit-identical vectors and ranks) at the same 16
+// warps per SM; capped below 128 registers (17 warps) it spilled and was
+// slower (120: 0.922 ms, 112: 0.947 ms). The packed batch kernel keeps the
+// two-row code, which its descriptor lookups leave fewer spills in.
 template <int TMAX>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(32, eigh_reg_min_blocks<TMAX>())
     eigh_reg_kernel(const float* gram, float* vecs, float* __restrict__ lam_out, int32_t* __restrict__ ranks,
                     float* __restrict__ wgt, float* __restrict__ sig2, int n, int nvox, long long patch0,
                     int* __restrict__ refine_count, int* __restrict__ refine_ids) {
